@@ -1,0 +1,141 @@
+/*
+ * mqp.h - C ABI of the B200-native cross-correlation PIV hot path.
+ *
+ * Drop-in boundary for multi_quickPIV (Julia).  The reference runs the whole
+ * PIV hot path in Julia and calls native code only through FFTW's @ccall
+ * (src/utils/fft_ops.jl:18-80).  Its user API is
+ *   PIV(img1, img2[, mask[, mask_IA]], pivparams; precision)
+ *   (src/multi_quickPIV.jl:17-29)
+ * built on setPIVParameters (src/piv_parameters.jl:67-81).  This library
+ * replaces the per-interrogation-area loop behind that API
+ * (src/multi_quickPIV.jl:57-93, i.e. allocate_tmp_data / prepare_inputs! /
+ * crosscorrelation! / gaussian_displacement / compute_SN per IA) with one
+ * call per image pair, so a Julia method
+ *   PIV(img1, img2, pivparams; backend=:b200)
+ * can ccall mqp_piv with the arrays it already holds.
+ *
+ * Conventions
+ *  - Arrays are column-major (Julia order).  dims[0] is Julia dimension 1.
+ *  - VF has shape (N, vf_1, ..., vf_N), component fastest, Float64, as
+ *    allocate_outputs (src/utils/piv_ops.jl:25-31) lays it out; SN has shape
+ *    (vf_1, ..., vf_N).  The caller owns every buffer it passes in.
+ *  - Every function returns MQP_OK (0) or a negative MQP_ERR_* code; the
+ *    message of the last failure on a context is mqp_last_error(ctx).
+ *    Nothing aborts the process.
+ *  - A context is bound to one CUDA device and owns its device buffers and
+ *    stream.  Calls on one context are serialised; use one context per host
+ *    thread for concurrency.
+ */
+#ifndef MQP_H
+#define MQP_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MQP_ABI_VERSION 1
+
+#if defined(_WIN32)
+#define MQP_API __declspec(dllexport)
+#else
+#define MQP_API __attribute__((visibility("default")))
+#endif
+
+/* status codes */
+#define MQP_OK 0
+#define MQP_ERR_INVALID (-1)     /* bad argument, shape or parameter */
+#define MQP_ERR_UNSUPPORTED (-2) /* valid in the reference but not on this path */
+#define MQP_ERR_CUDA (-3)        /* CUDA runtime failure */
+#define MQP_ERR_OOM (-4)         /* device allocation failed */
+#define MQP_ERR_TIMEOUT (-5)     /* a bounded device wait gave up */
+#define MQP_ERR_BUSY (-6)        /* admission refused (serving) */
+#define MQP_ERR_NOT_FOUND (-7)   /* unknown request / stream id */
+
+/* correlation algorithms: the CORRTYPES of src/piv_parameters.jl:1-6 */
+#define MQP_FFTCC 0
+#define MQP_ZNCC 1
+#define MQP_NSQECC 2
+#define MQP_MASK_NSQECC 3
+
+/* element types of the images (and mask) */
+#define MQP_F32 0
+#define MQP_F64 1
+
+/*
+ * PIVParameters (src/piv_parameters.jl:28-45) as a POD.  Fields hold the
+ * STORED values of the Julia struct, i.e. after setPIVParameters' positional
+ * constructor has swapped unpadded/good_pad (src/piv_parameters.jl:57-59).
+ * filtFun / mask_filtFun are fixed to maxval (Julia closures cannot cross
+ * the ABI).
+ */
+typedef struct mqp_params {
+  int32_t corr_alg;        /* MQP_FFTCC | MQP_ZNCC | MQP_NSQECC (mask given => masked NSQECC) */
+  int32_t interSize[3];    /* per Julia dimension */
+  int32_t searchMargin[3];
+  int32_t overlap[3];
+  int32_t step[3];         /* used when has_step != 0 */
+  int32_t has_step;        /* 0: step = interSize - overlap (src/piv_parameters.jl:87) */
+  int32_t multipass;       /* >= 1 */
+  int32_t computeSN;
+  int32_t unpadded;        /* stored value; must be 1 (src/utils/piv_ops.jl:257-268) */
+  int32_t good_pad;        /* stored value */
+  int32_t odd_pad;
+  double threshold;        /* skip IA when threshold >= 0 and maxval(IA) < threshold */
+  double mask_threshold;   /* masked PIV: skip when > 0 and maxval(mask IA) < it */
+  double ovp_th;           /* carried for completeness; unused by the reference kernels */
+  int32_t refine;          /* 0: multipass re-runs scale 1 (the reference); 1: predictor refinement */
+  int32_t reserved[7];
+} mqp_params;
+
+typedef struct mqp_ctx mqp_ctx;
+
+/* ABI version of the loaded library (MQP_ABI_VERSION). */
+MQP_API int mqp_abi_version(void);
+
+/* Create a context on CUDA device `device`.  Fails with MQP_ERR_CUDA when no
+ * such device exists. */
+MQP_API int mqp_create(mqp_ctx** out, int device);
+
+/* Release a context and its device memory. */
+MQP_API int mqp_destroy(mqp_ctx* ctx);
+
+/* Message of the last failing call on ctx (or of the last failing
+ * mqp_create when ctx is NULL).  Valid until the next call on ctx. */
+MQP_API const char* mqp_last_error(const mqp_ctx* ctx);
+
+/* get_vectorfield_size (src/utils/piv_ops.jl:6-14): vf_dims_out[d] for
+ * d < ndims (the rest set to 1). */
+MQP_API int mqp_vf_dims(const mqp_params* p, int ndims, const int64_t dims[3], int64_t vf_dims_out[3]);
+
+/* PIV on HOST arrays (src/multi_quickPIV.jl:17-29).  img1, img2 (and mask,
+ * nullable) are column-major arrays of `dtype` with extents dims[0..ndims).
+ * mask != NULL selects masked NSQECC; mask_skip (nullable) is the separate
+ * skip mask of the double-masked method (src/multi_quickPIV.jl:27-29).  VF
+ * receives N*prod(vf) doubles, SN (nullable; used when computeSN) prod(vf).
+ * Blocks until the result is in VF/SN. */
+MQP_API int mqp_piv(mqp_ctx* ctx, const void* img1, const void* img2, const void* mask,
+            const void* mask_skip, int dtype, int ndims, const int64_t dims[3],
+            const mqp_params* p, double* VF, double* SN, int64_t vf_dims_out[3]);
+
+/* The same on DEVICE arrays already resident in HBM, enqueued on `stream`
+ * (a cudaStream_t; NULL = the context's stream).  Returns once the work is
+ * enqueued; synchronise the stream before reading d_VF / d_SN. */
+MQP_API int mqp_piv_device(mqp_ctx* ctx, const void* d_img1, const void* d_img2, const void* d_mask,
+                   const void* d_mask_skip, int dtype, int ndims, const int64_t dims[3],
+                   const mqp_params* p, double* d_VF, double* d_SN, void* stream);
+
+/* Debug/test entry: the fully-overlapping similarity planes (the block
+ * tmp_data[1][1:2SM+1, ...] the reference searches, src/utils/piv_ops.jl:257-260)
+ * for the IAs [ia_begin, ia_end) of the vector field, written to the host
+ * buffer `planes` as (2SM1+1, 2SM2+1[, 2SM3+1], n) doubles. */
+MQP_API int mqp_correlation_planes(mqp_ctx* ctx, const void* img1, const void* img2, const void* mask,
+                           int dtype, int ndims, const int64_t dims[3], const mqp_params* p,
+                           int64_t ia_begin, int64_t ia_end, double* planes);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MQP_H */

@@ -1,0 +1,133 @@
+"""ctypes binding of the C ABI in include/mqp.h (libmqp_b200.so).
+
+The library is built in-tree by ``python -m multi_quickpiv_b200.build``.
+There is no fallback: when the library is missing, loading fails loudly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libmqp_b200.so")
+
+MQP_OK = 0
+MQP_ERR_INVALID = -1
+MQP_ERR_UNSUPPORTED = -2
+MQP_ERR_CUDA = -3
+MQP_ERR_OOM = -4
+MQP_ERR_TIMEOUT = -5
+MQP_ERR_BUSY = -6
+MQP_ERR_NOT_FOUND = -7
+
+MQP_FFTCC, MQP_ZNCC, MQP_NSQECC, MQP_MASK_NSQECC = 0, 1, 2, 3
+MQP_F32, MQP_F64 = 0, 1
+
+# every symbol declared in include/mqp.h, with its ctypes signature
+I64x3 = C.c_int64 * 3
+
+
+class MqpParams(C.Structure):
+    _fields_ = [
+        ("corr_alg", C.c_int32),
+        ("interSize", C.c_int32 * 3),
+        ("searchMargin", C.c_int32 * 3),
+        ("overlap", C.c_int32 * 3),
+        ("step", C.c_int32 * 3),
+        ("has_step", C.c_int32),
+        ("multipass", C.c_int32),
+        ("computeSN", C.c_int32),
+        ("unpadded", C.c_int32),
+        ("good_pad", C.c_int32),
+        ("odd_pad", C.c_int32),
+        ("threshold", C.c_double),
+        ("mask_threshold", C.c_double),
+        ("ovp_th", C.c_double),
+        ("refine", C.c_int32),
+        ("reserved", C.c_int32 * 7),
+    ]
+
+
+SIGNATURES = {
+    "mqp_abi_version": (C.c_int, []),
+    "mqp_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int]),
+    "mqp_destroy": (C.c_int, [C.c_void_p]),
+    "mqp_last_error": (C.c_char_p, [C.c_void_p]),
+    "mqp_vf_dims": (C.c_int, [C.POINTER(MqpParams), C.c_int, I64x3, I64x3]),
+    "mqp_piv": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                          I64x3, C.POINTER(MqpParams), C.c_void_p, C.c_void_p, I64x3]),
+    "mqp_piv_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                 I64x3, C.POINTER(MqpParams), C.c_void_p, C.c_void_p, C.c_void_p]),
+    "mqp_correlation_planes": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                         I64x3, C.POINTER(MqpParams), C.c_int64, C.c_int64, C.c_void_p]),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+class MQPError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[mqp {code}] {msg}")
+        self.code = code
+
+
+def load(path: str = LIB_PATH):
+    """Load libmqp_b200.so (cached).  Raises if it has not been built."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(path):
+            raise ImportError(f"native library {path} is missing: build it with "
+                              "`python -m multi_quickpiv_b200.build` (there is no CPU fallback)")
+        lib = C.CDLL(path)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+        return lib
+
+
+def check(rc: int, ctx=None):
+    if rc != MQP_OK:
+        lib = load()
+        msg = lib.mqp_last_error(ctx)
+        raise MQPError(rc, msg.decode() if msg else "unknown error")
+
+
+class Context:
+    """An mqp_ctx bound to one CUDA device (owns device buffers + a stream)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load()
+        h = C.c_void_p()
+        check(self.lib.mqp_create(C.byref(h), int(device)), None)
+        self.handle = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.mqp_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_ctx_cache = {}
+
+
+def default_context(device: int = 0) -> Context:
+    with _lock:
+        c = _ctx_cache.get(device)
+    if c is None:
+        c = Context(device)
+        with _lock:
+            _ctx_cache[device] = c
+    return c

@@ -1,0 +1,28 @@
+"""Builds tests/_native/libmqp_emu.so, the host emulation of the 2D kernel
+used by the CPU tests (see mqp_emu.cu)."""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+CSRC = os.path.join(ROOT, "multi_quickpiv_b200", "csrc")
+OUT = os.path.join(os.path.dirname(HERE), "_native", "libmqp_emu.so")
+
+
+def build(force=False):
+    src = os.path.join(HERE, "mqp_emu.cu")
+    deps = [src] + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".inc"))]
+    if not force and os.path.exists(OUT) and all(os.path.getmtime(d) <= os.path.getmtime(OUT) for d in deps):
+        return OUT
+    os.makedirs(os.path.dirname(OUT), exist_ok=True)
+    cmd = ["nvcc", "-std=c++17", "-O2", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-fvisibility=hidden",
+           "-shared", "-I", CSRC, src, "-o", OUT]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(r.stdout + r.stderr)
+    return OUT
+
+
+if __name__ == "__main__":
+    print(build("--force" in sys.argv))

@@ -1,0 +1,182 @@
+// Host emulation of the fused 2D kernel for CPU tests (test infrastructure,
+// not part of the product library).  It runs the SAME per-lane phase
+// functions as piv2d_kernel (mqp_piv2d.cuh), lane by lane, with the warp
+// reductions replaced by plain loops, so FFT indexing, scaling, window
+// geometry and peak logic can be checked against the oracle without a GPU.
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <vector>
+
+#include "mqp_piv2d.cuh"
+
+using namespace mqp;
+
+static void integral(const void* img, int dtype, int H, int W, bool sq, std::vector<double>& out) {
+  const long long ld = H + 1;
+  out.assign((size_t)ld * (W + 1), 0.0);
+  for (int c = 1; c <= W; ++c) {
+    double acc = 0.0;
+    for (int r = 1; r <= H; ++r) {
+      double v = load_px(img, dtype, (long long)(r - 1) + (long long)H * (c - 1));
+      if (sq) v = v * v;
+      acc += v;
+      out[r + ld * c] = out[r + ld * (c - 1)] + acc;
+    }
+  }
+}
+
+template <int N, bool FPRUNE, int ALG>
+static void emu_ia(const Piv2dArgs& a, long long ia, std::vector<float2>& ws) {
+  using Lay = Layout2d<N, FPRUNE>;
+  constexpr int M = N / 2;
+  const int P1 = 2 * a.SM1 + 1, P2 = 2 * a.SM2 + 1;
+  float2* GH = ws.data();
+  float2* FH = GH + Lay::F_OFF;
+  double* plane = reinterpret_cast<double*>(FH);
+  const int v1 = (int)(ia % a.vf1), v2 = (int)(ia / a.vf1);
+  int d1, d2;
+  ia_pred(a, v1, v2, d1, d2);
+  const IAGeom g = ia_geom(a, v1, v2);
+  IAScalars sc;
+  sc.meanF = sc.meanG = 0.0;
+  if (ALG == ALG_ZNCC) {
+    sc.meanF = box_sum(a.II1, a.H, g.ir1, g.ir1 + a.IS1, g.ir2, g.ir2 + a.IS2) / ((double)a.IS1 * a.IS2);
+    const double nG = (double)(g.hi1 - g.lo1) * (double)(g.hi2 - g.lo2);
+    sc.meanG = box_sum(a.IIg, a.H, g.g01 + g.lo1, g.g01 + g.hi1, g.g02 + g.lo2, g.g02 + g.hi2) / nG;
+  }
+  double vmax = -INFINITY, sumsq = 0.0, msum = 0.0;
+  for (int lane = 0; lane < 32; ++lane)
+    for (int x2 = lane; x2 < Lay::NF; x2 += 32) {
+      if (x2 < a.IS2) phase1_F_column<N, FPRUNE>(a, g, x2, sc.meanF, false, FH, vmax, sumsq, msum);
+      else zero_column(FH + x2, M, Lay::FSTR);
+    }
+  sc.sumF2 = sumsq;
+  const long long vfo = (long long)v1 + (long long)a.vf1 * v2;
+  if (a.threshold >= 0.0 && vmax < a.threshold) {
+    a.VF[2 * vfo] = 0.0;
+    a.VF[2 * vfo + 1] = 0.0;
+    if (a.SN) a.SN[vfo] = 0.0;
+    if (a.planes) memset(a.planes + (ia - a.ia_begin) * (long long)P1 * P2, 0, sizeof(double) * P1 * P2);
+    return;
+  }
+  for (int lane = 0; lane < 32; ++lane)
+    for (int x2 = lane; x2 < N; x2 += 32) phase1_G_column<N, FPRUNE>(a, g, x2, sc.meanG, false, GH);
+  for (int lane = 0; lane < 32; ++lane)
+    for (int u = lane; u < M; u += 32) phase2_row<N, FPRUNE>(u, P2, GH, FH);
+  const double scale = cc_scale<N>();
+  for (int lane = 0; lane < 32; ++lane)
+    for (int s2 = lane; s2 < P2; s2 += 32) {
+      float cc[N];
+      phase3_column<N, FPRUNE>(s2, GH, cc);
+      for (int s1 = 0; s1 < P1; ++s1) plane[s1 + P1 * s2] = similarity<ALG>(a, g, sc, s1, s2, (double)cc[s1] * scale);
+    }
+  const int lo1 = g.tlf1, hi1 = 2 * a.SM1 - g.brb1, lo2 = g.tlf2, hi2 = 2 * a.SM2 - g.brb2;
+  double best = 0.0;
+  int bidx = -1;
+  for (int lane = 0; lane < 32; ++lane) {
+    double lb = 0.0;
+    int li = -1;
+    for (int s2 = lane; s2 <= hi2; s2 += 32)
+      if (s2 >= lo2) peak_scan_column(plane, P1, s2, lo1, hi1, lb, li);
+    peak_merge(best, bidx, lb, li);
+  }
+  double sn = 0.0;
+  if (a.SN) {
+    const int shi1 = 2 * a.SM1 - 1 - g.brb1, shi2 = 2 * a.SM2 - 1 - g.brb2;
+    double smax = -INFINITY, ssum = 0.0;
+    for (int s2 = lo2; s2 <= shi2; ++s2)
+      for (int s1 = lo1; s1 <= shi1; ++s1) {
+        smax = nmax(smax, plane[s1 + P1 * s2]);
+        ssum += plane[s1 + P1 * s2];
+      }
+    const double len = (double)(shi1 - lo1 + 1) * (double)(shi2 - lo2 + 1);
+    sn = smax / ((ssum - smax) / (len - 1.0));
+  }
+  if (a.planes) memcpy(a.planes + (ia - a.ia_begin) * (long long)P1 * P2, plane, sizeof(double) * P1 * P2);
+  double r1 = -1.0, r2 = -1.0;
+  if (bidx >= 0) refine2d(plane, P1, a.SM1, a.SM2, g, bidx % P1, bidx / P1, best, r1, r2);
+  a.VF[2 * vfo] = r1 - a.SM1 + d1;
+  a.VF[2 * vfo + 1] = r2 - a.SM2 + d2;
+  if (a.SN) a.SN[vfo] = sn;
+}
+
+template <int N, bool FPRUNE, int ALG>
+static void emu_run(const Piv2dArgs& a) {
+  using Lay = Layout2d<N, FPRUNE>;
+  std::vector<float2> ws((size_t)Lay::warp_f2(2 * a.SM1 + 1, 2 * a.SM2 + 1));
+  for (long long ia = a.ia_begin; ia < a.ia_end; ++ia) emu_ia<N, FPRUNE, ALG>(a, ia, ws);
+}
+
+template <int N, bool FPRUNE>
+static int emu_alg(const Piv2dArgs& a, int alg) {
+  if (alg == 0) emu_run<N, FPRUNE, 0>(a);
+  else if (alg == 1) emu_run<N, FPRUNE, 1>(a);
+  else if (alg == 2) emu_run<N, FPRUNE, 2>(a);
+  else return -1;
+  return 0;
+}
+
+extern "C" __attribute__((visibility("default"))) int mqp_emu_piv2d(
+    const void* img1, const void* img2, int dtype, int H, int W, int IS1, int IS2, int SM1, int SM2,
+    int st1, int st2, int alg, double threshold, int computeSN, double* VF, double* SN, double* planes,
+    long long ia_begin, long long ia_end) {
+  std::vector<double> II1, IIg, IIg2;
+  Piv2dArgs a;
+  memset(&a, 0, sizeof(a));
+  a.img1 = img1;
+  a.img2 = img2;
+  a.dtype = dtype;
+  if (alg == 1 || alg == 2) {
+    integral(img2, dtype, H, W, true, IIg2);
+    a.IIg2 = IIg2.data();
+  }
+  if (alg == 1) {
+    integral(img2, dtype, H, W, false, IIg);
+    integral(img1, dtype, H, W, false, II1);
+    a.IIg = IIg.data();
+    a.II1 = II1.data();
+  }
+  a.VF = VF;
+  a.SN = computeSN ? SN : nullptr;
+  a.planes = planes;
+  a.H = H; a.W = W; a.IS1 = IS1; a.IS2 = IS2; a.SM1 = SM1; a.SM2 = SM2; a.st1 = st1; a.st2 = st2;
+  a.vf1 = (H - IS1) / st1 + 1;
+  a.vf2 = (W - IS2) / st2 + 1;
+  a.ia_begin = ia_begin;
+  a.ia_end = ia_end;
+  a.threshold = threshold;
+  a.computeSN = computeSN;
+  const int SS = (IS1 + 2 * SM1) > (IS2 + 2 * SM2) ? (IS1 + 2 * SM1) : (IS2 + 2 * SM2);
+  const int N = SS <= 32 ? 32 : (SS <= 64 ? 64 : 0);
+  const bool prune = IS1 <= N / 2 && IS2 <= N / 2;
+  if (N == 64) return prune ? emu_alg<64, true>(a, alg) : emu_alg<64, false>(a, alg);
+  if (N == 32) return prune ? emu_alg<32, true>(a, alg) : emu_alg<32, false>(a, alg);
+  return -2;
+}
+
+// one register FFT, for direct unit tests of mqp_fft.cuh
+extern "C" __attribute__((visibility("default"))) int mqp_emu_fft(int n, int inverse, float* io) {
+  auto run = [&](auto tag) {
+    constexpr int NN = decltype(tag)::value;
+    float2 x[NN];
+    for (int i = 0; i < NN; ++i) x[i] = make_float2(io[2 * i], io[2 * i + 1]);
+    if (inverse) fft_reg<NN, true>(x);
+    else fft_reg<NN, false>(x);
+    for (int k = 0; k < NN; ++k) {
+      io[2 * k] = x[fpos<NN>(k)].x;
+      io[2 * k + 1] = x[fpos<NN>(k)].y;
+    }
+  };
+  switch (n) {
+    case 4: run(std::integral_constant<int, 4>()); break;
+    case 8: run(std::integral_constant<int, 8>()); break;
+    case 16: run(std::integral_constant<int, 16>()); break;
+    case 32: run(std::integral_constant<int, 32>()); break;
+    case 64: run(std::integral_constant<int, 64>()); break;
+    case 128: run(std::integral_constant<int, 128>()); break;
+    default: return -1;
+  }
+  return 0;
+}
