@@ -120,8 +120,9 @@ MQP_API int mqp_piv(mqp_ctx* ctx, const void* img1, const void* img2, const void
             const mqp_params* p, double* VF, double* SN, int64_t vf_dims_out[3]);
 
 /* The same on DEVICE arrays already resident in HBM, enqueued on `stream`
- * (a cudaStream_t; NULL = the context's stream).  Returns once the work is
- * enqueued; synchronise the stream before reading d_VF / d_SN. */
+ * (a cudaStream_t; NULL = the legacy default stream, as in the CUDA
+ * runtime).  Returns once the work is enqueued; synchronise the stream
+ * before reading d_VF / d_SN. */
 MQP_API int mqp_piv_device(mqp_ctx* ctx, const void* d_img1, const void* d_img2, const void* d_mask,
                    const void* d_mask_skip, int dtype, int ndims, const int64_t dims[3],
                    const mqp_params* p, double* d_VF, double* d_SN, void* stream);
@@ -133,6 +134,22 @@ MQP_API int mqp_piv_device(mqp_ctx* ctx, const void* d_img1, const void* d_img2,
 MQP_API int mqp_correlation_planes(mqp_ctx* ctx, const void* img1, const void* img2, const void* mask,
                            int dtype, int ndims, const int64_t dims[3], const mqp_params* p,
                            int64_t ia_begin, int64_t ia_end, double* planes);
+
+/* Kernel timing (tracing).  While enabled, every kernel class is bracketed
+ * by CUDA events on the stream it is launched on; mqp_profile_read waits
+ * for the recorded work and returns the accumulated device times. */
+typedef struct mqp_profile {
+  int64_t launches_integral; /* integral-image scan kernels */
+  int64_t launches_piv;      /* fused correlation kernels */
+  int64_t launches_other;    /* predictor / post-processing kernels */
+  double ms_integral;
+  double ms_piv;
+  double ms_other;
+  int64_t ia_count;          /* interrogation areas processed by the fused kernels */
+} mqp_profile;
+
+MQP_API int mqp_profile_enable(mqp_ctx* ctx, int enable); /* also resets the counters */
+MQP_API int mqp_profile_read(mqp_ctx* ctx, mqp_profile* out);
 
 #ifdef __cplusplus
 }

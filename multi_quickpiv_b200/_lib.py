@@ -49,6 +49,18 @@ class MqpParams(C.Structure):
     ]
 
 
+class MqpProfile(C.Structure):
+    _fields_ = [
+        ("launches_integral", C.c_int64),
+        ("launches_piv", C.c_int64),
+        ("launches_other", C.c_int64),
+        ("ms_integral", C.c_double),
+        ("ms_piv", C.c_double),
+        ("ms_other", C.c_double),
+        ("ia_count", C.c_int64),
+    ]
+
+
 SIGNATURES = {
     "mqp_abi_version": (C.c_int, []),
     "mqp_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int]),
@@ -61,6 +73,8 @@ SIGNATURES = {
                                  I64x3, C.POINTER(MqpParams), C.c_void_p, C.c_void_p, C.c_void_p]),
     "mqp_correlation_planes": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
                                          I64x3, C.POINTER(MqpParams), C.c_int64, C.c_int64, C.c_void_p]),
+    "mqp_profile_enable": (C.c_int, [C.c_void_p, C.c_int]),
+    "mqp_profile_read": (C.c_int, [C.c_void_p, C.POINTER(MqpProfile)]),
 }
 
 _lib = None
@@ -107,6 +121,14 @@ class Context:
         check(self.lib.mqp_create(C.byref(h), int(device)), None)
         self.handle = h
         self.device = device
+
+    def profile_enable(self, on: bool = True):
+        check(self.lib.mqp_profile_enable(self.handle, int(on)), self.handle)
+
+    def profile_read(self) -> dict:
+        out = MqpProfile()
+        check(self.lib.mqp_profile_read(self.handle, C.byref(out)), self.handle)
+        return {f: getattr(out, f) for f, _ in MqpProfile._fields_}
 
     def close(self):
         if getattr(self, "handle", None):

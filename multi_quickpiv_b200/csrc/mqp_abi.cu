@@ -44,7 +44,40 @@ struct mqp_ctx {
   std::string last_error;
   std::mutex mu;
   DevBuf img1, img2, mask, mask_skip, II1, IIg, IIg2, VF, SN, pred, planes, status;
+  // tracing
+  bool profile = false;
+  struct Span {
+    cudaEvent_t a, b;
+    int kind;  // 0 integral, 1 piv, 2 other
+    int64_t ia;
+  };
+  std::vector<Span> spans;
+  mqp_profile prof{};
 };
+
+namespace {
+
+struct ProfileScope {
+  mqp_ctx* ctx;
+  cudaStream_t s;
+  mqp_ctx::Span sp{};
+  bool on;
+  ProfileScope(mqp_ctx* c, cudaStream_t st, int kind, int64_t ia) : ctx(c), s(st), on(c->profile) {
+    if (!on) return;
+    sp.kind = kind;
+    sp.ia = ia;
+    cudaEventCreate(&sp.a);
+    cudaEventCreate(&sp.b);
+    cudaEventRecord(sp.a, s);
+  }
+  ~ProfileScope() {
+    if (!on) return;
+    cudaEventRecord(sp.b, s);
+    ctx->spans.push_back(sp);
+  }
+};
+
+}  // namespace
 
 namespace {
 
@@ -189,12 +222,14 @@ int run_pass_2d(mqp_ctx* ctx, const Problem& pb, const mqp_params* p, const void
   a.img2 = d2;
   a.dtype = dtype;
   if (pb.alg == mqp::ALG_NSQECC || pb.alg == mqp::ALG_ZNCC) {
+    ProfileScope ps(ctx, s, 0, 0);
     if ((e = ctx->IIg2.ensure(ii_bytes)) != cudaSuccess) return cuda_fail(ctx, e, "integral buffer");
     if ((e = mqp::launch_integral2d(d2, dtype, H, W, true, (double*)ctx->IIg2.ptr, s)) != cudaSuccess)
       return cuda_fail(ctx, e, "integral image of img2^2");
     a.IIg2 = (const double*)ctx->IIg2.ptr;
   }
   if (pb.alg == mqp::ALG_ZNCC) {
+    ProfileScope ps(ctx, s, 0, 0);
     if ((e = ctx->IIg.ensure(ii_bytes)) != cudaSuccess) return cuda_fail(ctx, e, "integral buffer");
     if ((e = ctx->II1.ensure(ii_bytes)) != cudaSuccess) return cuda_fail(ctx, e, "integral buffer");
     if ((e = mqp::launch_integral2d(d2, dtype, H, W, false, (double*)ctx->IIg.ptr, s)) != cudaSuccess)
@@ -223,7 +258,10 @@ int run_pass_2d(mqp_ctx* ctx, const Problem& pb, const mqp_params* p, const void
   a.threshold = p->threshold;
   a.computeSN = dSN != nullptr;
   std::string err;
-  e = mqp::launch_piv2d(a, pb.alg, s, err);
+  {
+    ProfileScope ps(ctx, s, 1, ia_end - ia_begin);
+    e = mqp::launch_piv2d(a, pb.alg, s, err);
+  }
   if (e != cudaSuccess) return fail(ctx, e == cudaErrorInvalidValue ? MQP_ERR_UNSUPPORTED : MQP_ERR_CUDA, err);
   return MQP_OK;
 }
@@ -259,7 +297,7 @@ int mqp_piv_device(mqp_ctx* ctx, const void* d_img1, const void* d_img2, const v
   if (!ctx) return fail(nullptr, MQP_ERR_INVALID, "null context");
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device);
-  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  cudaStream_t s = stream ? (cudaStream_t)stream : cudaStreamLegacy;
   return piv_device_impl(ctx, d_img1, d_img2, d_mask, d_mask_skip, dtype, ndims, dims, p, d_VF, d_SN, s,
                          nullptr, 0, -1);
 }
@@ -340,6 +378,49 @@ int mqp_piv(mqp_ctx* ctx, const void* img1, const void* img2, const void* mask, 
             int64_t vf_dims_out[3]) {
   return host_roundtrip(ctx, img1, img2, mask, mask_skip, dtype, ndims, dims, p, VF, SN, vf_dims_out,
                         nullptr, 0, -1);
+}
+
+int mqp_profile_enable(mqp_ctx* ctx, int enable) {
+  if (!ctx) return fail(nullptr, MQP_ERR_INVALID, "null context");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  for (auto& sp : ctx->spans) {
+    cudaEventSynchronize(sp.b);
+    cudaEventDestroy(sp.a);
+    cudaEventDestroy(sp.b);
+  }
+  ctx->spans.clear();
+  ctx->prof = mqp_profile{};
+  ctx->profile = enable != 0;
+  return MQP_OK;
+}
+
+int mqp_profile_read(mqp_ctx* ctx, mqp_profile* out) {
+  if (!ctx || !out) return fail(ctx, MQP_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  for (auto& sp : ctx->spans) {
+    cudaError_t e = cudaEventSynchronize(sp.b);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "profile event");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, sp.a, sp.b);
+    if (sp.kind == 0) {
+      ctx->prof.launches_integral += 1;
+      ctx->prof.ms_integral += ms;
+    } else if (sp.kind == 1) {
+      ctx->prof.launches_piv += 1;
+      ctx->prof.ms_piv += ms;
+      ctx->prof.ia_count += sp.ia;
+    } else {
+      ctx->prof.launches_other += 1;
+      ctx->prof.ms_other += ms;
+    }
+    cudaEventDestroy(sp.a);
+    cudaEventDestroy(sp.b);
+  }
+  ctx->spans.clear();
+  *out = ctx->prof;
+  return MQP_OK;
 }
 
 int mqp_correlation_planes(mqp_ctx* ctx, const void* img1, const void* img2, const void* mask,

@@ -120,9 +120,9 @@ __device__ __forceinline__ void warp_peak(double& best, int& bidx) {
 // the fused kernel
 // ---------------------------------------------------------------------------
 // Persistent: each warp walks IAs ia = first + k * (all warps).  The warp's
-// shared-memory workspace holds the spectra rows of G (M x (N+1)) and F
-// (M x (NF+1)); after phase 2 the F rows are reused for the FP64 plane.
-template <int N, bool FPRUNE, int ALG, int WARPS, int MINB>
+// shared-memory workspace holds the spectra rows of G (N/2 x (N+1)) and F
+// (N/2 x (NF+1)); after phase 2 the F rows are reused for the FP64 plane.
+template <int N, bool FPRUNE, int ALG, typename T, int WARPS, int MINB>
 __global__ void __launch_bounds__(WARPS * 32, MINB) piv2d_kernel(Piv2dArgs a) {
   extern __shared__ float2 smem[];
   using Lay = Layout2d<N, FPRUNE>;
@@ -132,6 +132,9 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) piv2d_kernel(Piv2dArgs a) {
   float2* GH = smem + (size_t)warp * Lay::warp_f2(P1, P2);
   float2* FH = GH + Lay::F_OFF;
   double* plane = reinterpret_cast<double*>(FH);
+  float2* tw = smem + (size_t)WARPS * Lay::warp_f2(P1, P2);  // (cos, sin)(2 pi j / N)
+  for (int j = threadIdx.x; j < N; j += blockDim.x) tw[j] = twiddle_cs(j * (TW_N / N));
+  __syncthreads();
   const long long nwarps = (long long)gridDim.x * WARPS;
   const double scale = cc_scale<N>();
 
@@ -151,11 +154,13 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) piv2d_kernel(Piv2dArgs a) {
       sc.meanG = box_sum(a.IIg, a.H, g.g01 + g.lo1, g.g01 + g.hi1, g.g02 + g.lo2, g.g02 + g.hi2) / nG;
     }
 
-    // ---- phase 1: F columns (+ skip test), then G columns ----
-    double vmax = -INFINITY, sumsq = 0.0, msum = 0.0;
-    for (int x2 = lane; x2 < Lay::NF; x2 += 32) {
-      if (x2 < a.IS2) phase1_F_column<N, FPRUNE>(a, g, x2, sc.meanF, false, FH, vmax, sumsq, msum);
-      else zero_column(FH + x2, M, Lay::FSTR);
+    // ---- phase 1: F rows (+ skip test), then G rows; r2c along dim 2 ----
+    constexpr int NJF = (Lay::NF + 31) / 32, NJG = N / 32;
+    double vmax = -INFINITY, sumsq = 0.0;
+#pragma unroll 1
+    for (int job = 0; job < NJF; ++job) {
+      const int row = lane + 32 * job;
+      if (row < Lay::NF) phase1_row<N, FPRUNE, T, ALG == ALG_ZNCC>(a, g, sc, true, row, GH, FH, vmax, sumsq);
     }
     vmax = warp_max(vmax);
     sc.sumF2 = warp_sum(sumsq);
@@ -174,21 +179,34 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) piv2d_kernel(Piv2dArgs a) {
       __syncwarp();
       continue;
     }
-    for (int x2 = lane; x2 < N; x2 += 32) phase1_G_column<N, FPRUNE>(a, g, x2, sc.meanG, false, GH);
+#pragma unroll 1
+    for (int job = 0; job < NJG; ++job)
+      phase1_row<N, FPRUNE, T, ALG == ALG_ZNCC>(a, g, sc, false, lane + 32 * job, GH, FH, vmax, sumsq);
     __syncwarp();
 
-    // ---- phase 2: rows along dim 2, product, inverse along dim 2 ----
-    for (int u = lane; u < M; u += 32) phase2_row<N, FPRUNE>(u, P2, GH, FH);
+    // ---- phase 2: along dim 1 per spectrum row, product, inverse ----
+#pragma unroll 1
+    for (int u = lane; u < M; u += 32) phase2_row<N, FPRUNE>(u, P1, GH, FH);
     __syncwarp();
 
-    // ---- phase 3: c2r along dim 1 per lag column, similarity -> plane ----
-    for (int s2 = lane; s2 < P2; s2 += 32) {
+    // ---- phase 3: c2r along dim 2 per lag row, similarity -> plane ----
+    // rows [0, lane_rows) one per lane; a short tail of rows (2*SM1+1 just
+    // above 32) is computed by the whole warp, lanes over s2.
+    const int lane_rows = (P1 - 32 > 0 && P1 - 32 <= 4) ? 32 : P1;
+#pragma unroll 1
+    for (int s1 = lane; s1 < lane_rows; s1 += 32) {
       float cc[N];
-      phase3_column<N, FPRUNE>(s2, GH, cc);
+      phase3_row<N, FPRUNE>(s1, GH, cc);
 #pragma unroll
-      for (int s1 = 0; s1 < N; ++s1)
-        if (s1 < P1) plane[s1 + P1 * s2] = similarity<ALG>(a, g, sc, s1, s2, (double)cc[s1] * scale);
+      for (int s2 = 0; s2 < N; ++s2)
+        if (s2 < P2) plane[s1 + P1 * s2] = (double)cc[s2] * scale;
+      similarity_row<ALG>(a, g, sc, s1, P1, P2, plane);
     }
+#pragma unroll 1
+    for (int s1 = lane_rows; s1 < P1; ++s1)
+      for (int s2 = lane; s2 < P2; s2 += 32)
+        plane[s1 + P1 * s2] =
+            similarity_one<ALG>(a, g, sc, s1, s2, (double)tail_row_value<N, FPRUNE>(GH, tw, s1, s2) * scale);
     __syncwarp();
 
     // ---- peak (first_fullovp_peak), SN, Gaussian refinement ----
@@ -196,22 +214,32 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) piv2d_kernel(Piv2dArgs a) {
     const int lo2 = g.tlf2, hi2 = 2 * a.SM2 - g.brb2;
     double best = 0.0;
     int bidx = -1;
-    for (int s2 = lane; s2 <= hi2; s2 += 32)
-      if (s2 >= lo2) peak_scan_column(plane, P1, s2, lo1, hi1, best, bidx);
+    for (int s1 = lane; s1 < lane_rows && s1 <= hi1; s1 += 32)
+      if (s1 >= lo1) peak_scan_row(plane, P1, s1, lo2, hi2, best, bidx);
+    for (int s1 = lane_rows > lo1 ? lane_rows : lo1; s1 <= hi1; ++s1)
+      for (int s2 = lane; s2 <= hi2; s2 += 32)
+        if (s2 >= lo2) peak_take(plane[s1 + P1 * s2], s1 + P1 * s2, best, bidx);
     warp_peak(best, bidx);
     double sn = 0.0;
     if (a.SN) {
       // compute_SN (src/utils/piv_ops.jl:336-367) over [TLF_off, 2SM-1-BRB_off]
       const int shi1 = 2 * a.SM1 - 1 - g.brb1, shi2 = 2 * a.SM2 - 1 - g.brb2;
       double smax = -INFINITY, ssum = 0.0;
-      for (int s2 = lane; s2 <= shi2; s2 += 32) {
-        if (s2 < lo2) continue;
-        for (int s1 = lo1; s1 <= shi1; ++s1) {
+      for (int s1 = lane; s1 < lane_rows && s1 <= shi1; s1 += 32) {
+        if (s1 < lo1) continue;
+        for (int s2 = lo2; s2 <= shi2; ++s2) {
           const double v = plane[s1 + P1 * s2];
           smax = nmax(smax, v);
           ssum += v;
         }
       }
+      for (int s1 = lane_rows > lo1 ? lane_rows : lo1; s1 <= shi1; ++s1)
+        for (int s2 = lane; s2 <= shi2; s2 += 32) {
+          if (s2 < lo2) continue;
+          const double v = plane[s1 + P1 * s2];
+          smax = nmax(smax, v);
+          ssum += v;
+        }
       smax = warp_nmax(smax);
       ssum = warp_sum(ssum);
       const double len = (double)(shi1 - lo1 + 1) * (double)(shi2 - lo2 + 1);
@@ -253,12 +281,12 @@ int device_sm_count(int device) {
   return n;
 }
 
-template <int N, bool FPRUNE, int ALG, int WARPS, int MINB>
+template <int N, bool FPRUNE, int ALG, typename T, int WARPS, int MINB>
 static cudaError_t launch_t(const Piv2dArgs& a, cudaStream_t s, std::string& err) {
   using Lay = Layout2d<N, FPRUNE>;
   const int P1 = 2 * a.SM1 + 1, P2 = 2 * a.SM2 + 1;
-  const size_t smem = (size_t)WARPS * Lay::warp_f2(P1, P2) * sizeof(float2);
-  auto kern = piv2d_kernel<N, FPRUNE, ALG, WARPS, MINB>;
+  const size_t smem = ((size_t)WARPS * Lay::warp_f2(P1, P2) + N) * sizeof(float2);
+  auto kern = piv2d_kernel<N, FPRUNE, ALG, T, WARPS, MINB>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) {
     err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e);
@@ -283,26 +311,28 @@ static cudaError_t launch_t(const Piv2dArgs& a, cudaStream_t s, std::string& err
   return e;
 }
 
-template <int N, bool FPRUNE, int WARPS, int MINB>
+template <int N, bool FPRUNE, typename T, int WARPS, int MINB>
 static cudaError_t launch_alg(const Piv2dArgs& a, int alg, cudaStream_t s, std::string& err) {
   switch (alg) {
-    case ALG_FFTCC: return launch_t<N, FPRUNE, ALG_FFTCC, WARPS, MINB>(a, s, err);
-    case ALG_ZNCC: return launch_t<N, FPRUNE, ALG_ZNCC, WARPS, MINB>(a, s, err);
-    case ALG_NSQECC: return launch_t<N, FPRUNE, ALG_NSQECC, WARPS, MINB>(a, s, err);
+    case ALG_FFTCC: return launch_t<N, FPRUNE, ALG_FFTCC, T, WARPS, MINB>(a, s, err);
+    case ALG_ZNCC: return launch_t<N, FPRUNE, ALG_ZNCC, T, WARPS, MINB>(a, s, err);
+    case ALG_NSQECC: return launch_t<N, FPRUNE, ALG_NSQECC, T, WARPS, MINB>(a, s, err);
     default: err = "unknown correlation algorithm"; return cudaErrorInvalidValue;
   }
+}
+
+template <int N, bool FPRUNE, int WARPS, int MINB>
+static cudaError_t launch_dt(const Piv2dArgs& a, int alg, cudaStream_t s, std::string& err) {
+  return a.dtype == 0 ? launch_alg<N, FPRUNE, float, WARPS, MINB>(a, alg, s, err)
+                      : launch_alg<N, FPRUNE, double, WARPS, MINB>(a, alg, s, err);
 }
 
 cudaError_t launch_piv2d(const Piv2dArgs& a, int alg, cudaStream_t s, std::string& err) {
   const int SS1 = a.IS1 + 2 * a.SM1, SS2 = a.IS2 + 2 * a.SM2;
   const int N = piv2d_fft_len(SS1, SS2);
   const bool prune = (a.IS1 <= N / 2) && (a.IS2 <= N / 2);
-  if (N == 64) {
-    return prune ? launch_alg<64, true, 4, 2>(a, alg, s, err) : launch_alg<64, false, 4, 2>(a, alg, s, err);
-  }
-  if (N == 32) {
-    return prune ? launch_alg<32, true, 8, 2>(a, alg, s, err) : launch_alg<32, false, 8, 2>(a, alg, s, err);
-  }
+  if (N == 64) return prune ? launch_dt<64, true, 4, 2>(a, alg, s, err) : launch_dt<64, false, 4, 2>(a, alg, s, err);
+  if (N == 32) return prune ? launch_dt<32, true, 4, 2>(a, alg, s, err) : launch_dt<32, false, 4, 2>(a, alg, s, err);
   err = "search window larger than 64 along some axis is not supported by the 2D kernel";
   return cudaErrorInvalidValue;
 }

@@ -1,0 +1,45 @@
+"""Shared comparison helpers for the parity tests."""
+import numpy as np
+
+import oracle.piv_oracle as O
+
+# FP32 FFT + FP64 normalisation vs Float64 ("Precision"):
+PLANE_RTOL = 2e-6      # |plane - oracle| <= PLANE_RTOL * max|oracle plane| on the searched lags
+VF_ATOL = 1e-3         # px, whenever the integer peak agrees
+SN_RTOL = 1e-4         # plus the conditioning term |SN|^2/|max| * 1e-6
+
+
+def searched_region(shape, IS, SM, st, k):
+    """Lag box [TLF_off, 2SM - BRB_off] the reference searches for IA k
+    (0-based vector-field coordinates), as slices."""
+    vf = O.get_vectorfield_size(shape, IS, st)
+    lin = int(np.ravel_multi_index(k, vf, order="F")) + 1
+    c = O.coords_for(lin, vf, shape, np.asarray(IS), np.asarray(SM), np.asarray(st))
+    return tuple(slice(int(t), 2 * int(m) - int(b) + 1) for t, m, b in zip(c[4], SM, c[5]))
+
+
+def compare_planes(planes, oracle_corr, shape, IS, SM, st):
+    """Max relative plane error on the searched lags, and a per-IA near-tie
+    flag (top two oracle candidates closer than the FP32 error bound)."""
+    vf = O.get_vectorfield_size(shape, IS, st)
+    worst = 0.0
+    near_tie = np.zeros(vf, dtype=bool)
+    for k, cm in oracle_corr.items():
+        ia = int(np.ravel_multi_index(k, vf, order="F"))
+        reg = searched_region(shape, IS, SM, st, k)
+        a = planes[..., ia][reg]
+        b = cm[reg]
+        if b.size == 0:
+            continue
+        scale = np.nanmax(np.abs(b))
+        fin = np.isfinite(b)
+        assert np.array_equal(fin, np.isfinite(a)), f"non-finite lags differ at IA {k}"
+        worst = max(worst, float(np.max(np.abs(a[fin] - b[fin]))) / scale)
+        v = np.sort(b[fin].ravel())[::-1]
+        near_tie[k] = v.size > 1 and (v[0] - v[1]) <= 4 * PLANE_RTOL * scale
+    return worst, near_tie
+
+
+def sn_ok(SN, SNo):
+    tol = SN_RTOL * np.abs(SNo) + SNo ** 2 * 1e-6
+    return (np.abs(SN - SNo) <= tol) | ~np.isfinite(SNo)

@@ -27,7 +27,7 @@ static void integral(const void* img, int dtype, int H, int W, bool sq, std::vec
   }
 }
 
-template <int N, bool FPRUNE, int ALG>
+template <int N, bool FPRUNE, int ALG, typename T>
 static void emu_ia(const Piv2dArgs& a, long long ia, std::vector<float2>& ws) {
   using Lay = Layout2d<N, FPRUNE>;
   constexpr int M = N / 2;
@@ -46,12 +46,9 @@ static void emu_ia(const Piv2dArgs& a, long long ia, std::vector<float2>& ws) {
     const double nG = (double)(g.hi1 - g.lo1) * (double)(g.hi2 - g.lo2);
     sc.meanG = box_sum(a.IIg, a.H, g.g01 + g.lo1, g.g01 + g.hi1, g.g02 + g.lo2, g.g02 + g.hi2) / nG;
   }
-  double vmax = -INFINITY, sumsq = 0.0, msum = 0.0;
-  for (int lane = 0; lane < 32; ++lane)
-    for (int x2 = lane; x2 < Lay::NF; x2 += 32) {
-      if (x2 < a.IS2) phase1_F_column<N, FPRUNE>(a, g, x2, sc.meanF, false, FH, vmax, sumsq, msum);
-      else zero_column(FH + x2, M, Lay::FSTR);
-    }
+  double vmax = -INFINITY, sumsq = 0.0;
+  for (int row = 0; row < Lay::NF; ++row)
+    phase1_row<N, FPRUNE, T, ALG == ALG_ZNCC>(a, g, sc, true, row, GH, FH, vmax, sumsq);
   sc.sumF2 = sumsq;
   const long long vfo = (long long)v1 + (long long)a.vf1 * v2;
   if (a.threshold >= 0.0 && vmax < a.threshold) {
@@ -61,25 +58,34 @@ static void emu_ia(const Piv2dArgs& a, long long ia, std::vector<float2>& ws) {
     if (a.planes) memset(a.planes + (ia - a.ia_begin) * (long long)P1 * P2, 0, sizeof(double) * P1 * P2);
     return;
   }
-  for (int lane = 0; lane < 32; ++lane)
-    for (int x2 = lane; x2 < N; x2 += 32) phase1_G_column<N, FPRUNE>(a, g, x2, sc.meanG, false, GH);
-  for (int lane = 0; lane < 32; ++lane)
-    for (int u = lane; u < M; u += 32) phase2_row<N, FPRUNE>(u, P2, GH, FH);
+  for (int row = 0; row < N; ++row)
+    phase1_row<N, FPRUNE, T, ALG == ALG_ZNCC>(a, g, sc, false, row, GH, FH, vmax, sumsq);
+  for (int u = 0; u < M; ++u) phase2_row<N, FPRUNE>(u, P1, GH, FH);
   const double scale = cc_scale<N>();
-  for (int lane = 0; lane < 32; ++lane)
-    for (int s2 = lane; s2 < P2; s2 += 32) {
-      float cc[N];
-      phase3_column<N, FPRUNE>(s2, GH, cc);
-      for (int s1 = 0; s1 < P1; ++s1) plane[s1 + P1 * s2] = similarity<ALG>(a, g, sc, s1, s2, (double)cc[s1] * scale);
-    }
+  const int lane_rows = (P1 - 32 > 0 && P1 - 32 <= 4) ? 32 : P1;
+  for (int s1 = 0; s1 < lane_rows; ++s1) {
+    float cc[N];
+    phase3_row<N, FPRUNE>(s1, GH, cc);
+    for (int s2 = 0; s2 < P2; ++s2) plane[s1 + P1 * s2] = (double)cc[s2] * scale;
+  }
+  for (int s1 = 0; s1 < lane_rows; ++s1) similarity_row<ALG>(a, g, sc, s1, P1, P2, plane);
+  float2 tw[N];
+  for (int j = 0; j < N; ++j) tw[j] = twiddle_cs(j * (TW_N / N));
+  for (int s1 = lane_rows; s1 < P1; ++s1)
+    for (int s2 = 0; s2 < P2; ++s2)
+      plane[s1 + P1 * s2] =
+          similarity_one<ALG>(a, g, sc, s1, s2, (double)tail_row_value<N, FPRUNE>(GH, tw, s1, s2) * scale);
   const int lo1 = g.tlf1, hi1 = 2 * a.SM1 - g.brb1, lo2 = g.tlf2, hi2 = 2 * a.SM2 - g.brb2;
   double best = 0.0;
   int bidx = -1;
   for (int lane = 0; lane < 32; ++lane) {
     double lb = 0.0;
     int li = -1;
-    for (int s2 = lane; s2 <= hi2; s2 += 32)
-      if (s2 >= lo2) peak_scan_column(plane, P1, s2, lo1, hi1, lb, li);
+    for (int s1 = lane; s1 < lane_rows && s1 <= hi1; s1 += 32)
+      if (s1 >= lo1) peak_scan_row(plane, P1, s1, lo2, hi2, lb, li);
+    for (int s1 = lane_rows > lo1 ? lane_rows : lo1; s1 <= hi1; ++s1)
+      for (int s2 = lane; s2 <= hi2; s2 += 32)
+        if (s2 >= lo2) peak_take(plane[s1 + P1 * s2], s1 + P1 * s2, lb, li);
     peak_merge(best, bidx, lb, li);
   }
   double sn = 0.0;
@@ -106,7 +112,10 @@ template <int N, bool FPRUNE, int ALG>
 static void emu_run(const Piv2dArgs& a) {
   using Lay = Layout2d<N, FPRUNE>;
   std::vector<float2> ws((size_t)Lay::warp_f2(2 * a.SM1 + 1, 2 * a.SM2 + 1));
-  for (long long ia = a.ia_begin; ia < a.ia_end; ++ia) emu_ia<N, FPRUNE, ALG>(a, ia, ws);
+  for (long long ia = a.ia_begin; ia < a.ia_end; ++ia) {
+    if (a.dtype == 0) emu_ia<N, FPRUNE, ALG, float>(a, ia, ws);
+    else emu_ia<N, FPRUNE, ALG, double>(a, ia, ws);
+  }
 }
 
 template <int N, bool FPRUNE>

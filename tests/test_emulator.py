@@ -1,0 +1,75 @@
+"""CPU check of the fused 2D kernel's logic: tests/native/mqp_emu.cu runs the
+kernel's own per-lane phase functions (register FFTs, staging, r2c/c2r
+splits, window geometry, normalisation, peak, Gaussian fit, SN) on the host."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle.piv_oracle as O
+from multi_quickpiv_b200 import synth
+from tests.helpers import PLANE_RTOL, VF_ATOL, compare_planes, sn_ok
+from tests.native import build_emu
+
+ALG = {"fft": 0, "zncc": 1, "nsqecc": 2}
+
+
+@pytest.fixture(scope="module")
+def emu():
+    return C.CDLL(build_emu.build())
+
+
+@pytest.mark.parametrize("n", [4, 8, 16, 32, 64, 128])
+def test_register_fft(emu, n):
+    g = np.random.default_rng(n)
+    x = (g.normal(size=n) + 1j * g.normal(size=n)).astype(np.complex64)
+    for inv in (0, 1):
+        io = np.stack([x.real, x.imag], -1).astype(np.float32).ravel().copy()
+        assert emu.mqp_emu_fft(n, inv, io.ctypes.data_as(C.c_void_p)) == 0
+        y = io[0::2] + 1j * io[1::2]
+        ref = np.fft.ifft(x.astype(np.complex128)) * n if inv else np.fft.fft(x.astype(np.complex128))
+        assert np.max(np.abs(y - ref)) / np.max(np.abs(ref)) < 3e-7
+
+
+def run_emu(emu, i1, i2, alg, IS, SM, st, thr=-1.0):
+    vf = O.get_vectorfield_size(i1.shape, IS, st)
+    n = vf[0] * vf[1]
+    P1, P2 = 2 * SM[0] + 1, 2 * SM[1] + 1
+    VF = np.zeros((2,) + vf, order="F")
+    SN = np.zeros(vf, order="F")
+    PL = np.zeros((P1, P2, n), order="F")
+    dt = 1 if i1.dtype == np.float64 else 0
+    f1, f2 = np.asfortranarray(i1), np.asfortranarray(i2)
+    p = lambda a: a.ctypes.data_as(C.c_void_p)
+    rc = emu.mqp_emu_piv2d(p(f1), p(f2), dt, i1.shape[0], i1.shape[1], IS[0], IS[1], SM[0], SM[1], st[0], st[1],
+                           ALG[alg], C.c_double(thr), 1, p(VF), p(SN), p(PL), C.c_longlong(0), C.c_longlong(n))
+    assert rc == 0
+    return VF, SN, PL
+
+
+@pytest.mark.parametrize("alg", ["fft", "zncc", "nsqecc"])
+@pytest.mark.parametrize("cfg", [((32, 32), (16, 16), (16, 16)), ((16, 16), (8, 8), (8, 8)),
+                                 ((32, 32), (10, 10), (16, 16)), ((24, 32), (12, 8), (12, 10)),
+                                 ((8, 12), (20, 18), (12, 12)), ((40, 36), (12, 14), (16, 16))])
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_emulated_kernel_matches_oracle(emu, alg, cfg, dtype):
+    IS, SM, st = cfg
+    i1, i2, _ = synth.pair_2d_shift(shape=(112, 100), seed_stream=21)
+    i1, i2 = i1.astype(dtype), i2.astype(dtype)
+    po = O.set_piv_parameters(corr_alg=alg, interSize=IS, searchMargin=SM, step=st, computeSN=True)
+    po.ndims = 2
+    VFo, SNo, Co = O.piv_single_pass(i1, i2, po, keep_corr=True)
+    VF, SN, PL = run_emu(emu, i1, i2, alg, IS, SM, st)
+    worst, near_tie = compare_planes(PL, Co, i1.shape, IS, SM, st)
+    assert worst <= PLANE_RTOL, worst
+    bad = (np.abs(VF - VFo) > VF_ATOL).any(axis=0) & ~near_tie
+    assert not bad.any()
+    assert (sn_ok(SN, SNo) | near_tie).all()
+
+
+def test_emulated_threshold_skip(emu):
+    i1, i2, _ = synth.pair_2d_shift(shape=(96, 96))
+    i1 = i1.copy()
+    i1[:40, :40] = -10.0
+    VF, SN, _ = run_emu(emu, i1, i2, "fft", (32, 32), (16, 16), (16, 16), thr=0.0)
+    assert np.all(VF[:, 0, 0] == 0) and SN[0, 0] == 0

@@ -1,0 +1,71 @@
+"""GPU parity of the fused 2D kernel against the Float64 oracle, through the
+C ABI (multi_quickpiv_b200.PIV -> mqp_piv)."""
+import numpy as np
+import pytest
+
+import oracle.piv_oracle as O
+from multi_quickpiv_b200 import PIV, correlation_planes, setPIVParameters, synth
+from tests.helpers import PLANE_RTOL, VF_ATOL, compare_planes, sn_ok
+
+pytestmark = pytest.mark.gpu
+
+def _oracle_params(alg, IS, SM, st, thr=-1.0, sn=True):
+    p = O.set_piv_parameters(corr_alg=alg, interSize=IS, searchMargin=SM, step=st, computeSN=sn, threshold=thr)
+    p.ndims = len(IS)
+    return p
+
+
+def _compare(img1, img2, alg, IS, SM, st, thr=-1.0):
+    po = _oracle_params(alg, IS, SM, st, thr)
+    VFo, SNo, Co = O.piv_single_pass(img1, img2, po, keep_corr=True)
+    pp = setPIVParameters(corr_alg=alg, interSize=IS, searchMargin=SM, step=st, computeSN=True, threshold=thr)
+    VF, SN = PIV(img1, img2, pp)
+    assert VF.shape == VFo.shape and SN.shape == SNo.shape
+    planes = correlation_planes(img1, img2, pp)
+    worst, near_tie = compare_planes(planes, Co, img1.shape, IS, SM, st)
+    assert worst <= PLANE_RTOL, worst
+    bad = (np.abs(VF - VFo) > VF_ATOL).any(axis=0) & ~near_tie
+    assert not bad.any(), (np.argwhere(bad)[:5], np.abs(VF - VFo).max())
+    assert (sn_ok(SN, SNo) | near_tie).all()
+    return VF, VFo
+
+
+@pytest.mark.parametrize("alg", ["fft", "zncc", "nsqecc"])
+@pytest.mark.parametrize("cfg", [((32, 32), (16, 16), (16, 16)), ((16, 16), (8, 8), (8, 8)),
+                                 ((32, 32), (10, 10), (16, 16)), ((24, 32), (12, 8), (12, 10)),
+                                 ((8, 12), (20, 18), (12, 12)), ((40, 36), (12, 14), (16, 16))])
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_piv2d_matches_oracle(alg, cfg, dtype, gpu):
+    i1, i2, _ = synth.pair_2d_shift(shape=(160, 144))
+    _compare(i1.astype(dtype), i2.astype(dtype), alg, *cfg)
+
+
+def test_shift_workload_256_fftcc(gpu):
+    """The 256x256 Float64 FFTCC workload with threshold 0 and SN."""
+    i1, i2, shift = synth.pair_2d_shift()
+    VF, VFo = _compare(i1, i2, "fft", (32, 32), (16, 16), (16, 16), thr=0.0)
+    # interior vectors recover the imposed shift
+    inner = VF[:, 2:-2, 2:-2]
+    assert np.abs(np.median(inner[0]) - shift[0]) < 0.1
+    assert np.abs(np.median(inner[1]) - shift[1]) < 0.1
+
+
+@pytest.mark.parametrize("alg", ["zncc", "nsqecc"])
+def test_vortex_crop_float32(alg, gpu):
+    i1, i2, _ = synth.pair_2d_vortex(shape=(256, 320), core=60.0)
+    _compare(i1, i2, alg, (32, 32), (16, 16), (8, 8))
+
+
+def test_threshold_skip_leaves_zeros(gpu):
+    i1, i2, _ = synth.pair_2d_shift(shape=(128, 128))
+    i1 = i1.copy()
+    i1[:48, :48] = -100.0  # IAs fully inside stay below the threshold
+    VF, VFo = _compare(i1, i2, "fft", (32, 32), (16, 16), (16, 16), thr=0.0)
+    assert np.all(VF[:, 0, 0] == 0.0) and np.all(VFo[:, 0, 0] == 0.0)
+
+
+def test_float32_precision_output(gpu):
+    i1, i2, _ = synth.pair_2d_shift(shape=(96, 96))
+    pp = setPIVParameters(corr_alg="fft", interSize=(32, 32), searchMargin=(16, 16), step=(16, 16))
+    VF, SN = PIV(i1, i2, pp, precision=np.float32)
+    assert VF.dtype == np.float32 and SN is None
