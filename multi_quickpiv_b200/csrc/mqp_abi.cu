@@ -43,7 +43,7 @@ struct mqp_ctx {
   cudaStream_t stream = nullptr;
   std::string last_error;
   std::mutex mu;
-  DevBuf img1, img2, mask, mask_skip, II1, IIg, IIg2, VF, SN, pred, planes, status;
+  DevBuf img1, img2, mask, mask_skip, II1, IIg, IIg2, VF, SN, pred, planes, status, iscratch;
   // tracing
   bool profile = false;
   struct Span {
@@ -176,7 +176,7 @@ int mqp_destroy(mqp_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (DevBuf* b : {&ctx->img1, &ctx->img2, &ctx->mask, &ctx->mask_skip, &ctx->II1, &ctx->IIg, &ctx->IIg2,
-                    &ctx->VF, &ctx->SN, &ctx->pred, &ctx->planes, &ctx->status})
+                    &ctx->VF, &ctx->SN, &ctx->pred, &ctx->planes, &ctx->status, &ctx->iscratch})
     b->release();
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -222,9 +222,14 @@ int run_pass_2d(mqp_ctx* ctx, const Problem& pb, const mqp_params* p, const void
   a.img2 = d2;
   a.dtype = dtype;
   if (pb.alg == mqp::ALG_NSQECC || pb.alg == mqp::ALG_ZNCC) {
+    if ((e = ctx->iscratch.ensure(mqp::integral2d_scratch_bytes(H, W))) != cudaSuccess)
+      return cuda_fail(ctx, e, "integral scratch");
+  }
+  double* isc = (double*)ctx->iscratch.ptr;
+  if (pb.alg == mqp::ALG_NSQECC || pb.alg == mqp::ALG_ZNCC) {
     ProfileScope ps(ctx, s, 0, 0);
     if ((e = ctx->IIg2.ensure(ii_bytes)) != cudaSuccess) return cuda_fail(ctx, e, "integral buffer");
-    if ((e = mqp::launch_integral2d(d2, dtype, H, W, true, (double*)ctx->IIg2.ptr, s)) != cudaSuccess)
+    if ((e = mqp::launch_integral2d(d2, dtype, H, W, true, (double*)ctx->IIg2.ptr, isc, s)) != cudaSuccess)
       return cuda_fail(ctx, e, "integral image of img2^2");
     a.IIg2 = (const double*)ctx->IIg2.ptr;
   }
@@ -232,9 +237,9 @@ int run_pass_2d(mqp_ctx* ctx, const Problem& pb, const mqp_params* p, const void
     ProfileScope ps(ctx, s, 0, 0);
     if ((e = ctx->IIg.ensure(ii_bytes)) != cudaSuccess) return cuda_fail(ctx, e, "integral buffer");
     if ((e = ctx->II1.ensure(ii_bytes)) != cudaSuccess) return cuda_fail(ctx, e, "integral buffer");
-    if ((e = mqp::launch_integral2d(d2, dtype, H, W, false, (double*)ctx->IIg.ptr, s)) != cudaSuccess)
+    if ((e = mqp::launch_integral2d(d2, dtype, H, W, false, (double*)ctx->IIg.ptr, isc, s)) != cudaSuccess)
       return cuda_fail(ctx, e, "integral image of img2");
-    if ((e = mqp::launch_integral2d(d1, dtype, H, W, false, (double*)ctx->II1.ptr, s)) != cudaSuccess)
+    if ((e = mqp::launch_integral2d(d1, dtype, H, W, false, (double*)ctx->II1.ptr, isc, s)) != cudaSuccess)
       return cuda_fail(ctx, e, "integral image of img1");
     a.IIg = (const double*)ctx->IIg.ptr;
     a.II1 = (const double*)ctx->II1.ptr;

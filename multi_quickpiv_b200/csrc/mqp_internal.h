@@ -11,9 +11,11 @@
 namespace mqp {
 
 // FP64 exclusive-prefix integral image of img (or img^2) for a column-major
-// H x W image: out is (H+1) x (W+1), first row/column zero.
+// H x W image: out is (H+1) x (W+1), first row/column zero.  scratch holds
+// integral2d_scratch_bytes(H, W) bytes of per-chunk totals.
 cudaError_t launch_integral2d(const void* img, int dtype, int H, int W, bool square,
-                              double* out, cudaStream_t s);
+                              double* out, double* scratch, cudaStream_t s);
+size_t integral2d_scratch_bytes(int H, int W);
 
 // Smallest supported power-of-two FFT length covering the search window,
 // or 0 when the window is too large for the fused 2D kernel.

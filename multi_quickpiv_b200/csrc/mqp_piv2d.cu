@@ -50,32 +50,54 @@ __global__ void integral_cols_kernel(const T* __restrict__ img, int H, int W, do
   }
 }
 
-// pass 2: one thread per row of out, running sum across columns (dim 2);
-// consecutive threads read consecutive rows, so every step is coalesced.
-__global__ void integral_rows_kernel(int H, int W, double* __restrict__ out) {
+// pass 2: running sums across columns (dim 2) in chunks of ICHUNK columns:
+// thread (row r, chunk k) scans its chunk in place and records the chunk
+// total; consecutive threads take consecutive rows, so every step is a
+// coalesced column segment.
+constexpr int ICHUNK = 64;
+
+__global__ void integral_rows_chunk_kernel(int H, int W, double* __restrict__ out, double* __restrict__ totals) {
   const long long ld = (long long)H + 1;
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = blockIdx.y;
   if (r > H) return;
+  const int c0 = 1 + k * ICHUNK;
+  const int c1 = c0 + ICHUNK <= W + 1 ? c0 + ICHUNK : W + 1;
   double acc = 0.0;
-  int c = 1;
-  for (; c + 8 <= W + 1; c += 8) {
+  int c = c0;
+  for (; c + 8 <= c1; c += 8) {
     double v[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) v[k] = out[r + ld * (c + k)];
+    for (int t = 0; t < 8; ++t) v[t] = out[r + ld * (c + t)];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      acc += v[k];
-      out[r + ld * (c + k)] = acc;
+    for (int t = 0; t < 8; ++t) {
+      acc += v[t];
+      out[r + ld * (c + t)] = acc;
     }
   }
-  for (; c <= W; ++c) {
+  for (; c < c1; ++c) {
     acc += out[r + ld * c];
     out[r + ld * c] = acc;
   }
+  totals[r + ld * k] = acc;
+}
+
+// pass 3: every chunk k > 0 adds the sum of the totals of chunks 0..k-1
+__global__ void integral_rows_offset_kernel(int H, int W, double* __restrict__ out,
+                                            const double* __restrict__ totals) {
+  const long long ld = (long long)H + 1;
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = blockIdx.y + 1;
+  if (r > H) return;
+  double off = 0.0;
+  for (int q = 0; q < k; ++q) off += totals[r + ld * q];
+  const int c0 = 1 + k * ICHUNK;
+  const int c1 = c0 + ICHUNK <= W + 1 ? c0 + ICHUNK : W + 1;
+  for (int c = c0; c < c1; ++c) out[r + ld * c] += off;
 }
 
 cudaError_t launch_integral2d(const void* img, int dtype, int H, int W, bool square, double* out,
-                              cudaStream_t s) {
+                              double* scratch, cudaStream_t s) {
   const int threads = 256;
   const int blocks = (W + 1 + 7) / 8 < 4096 ? (W + 1 + 7) / 8 : 4096;
   if (dtype == 0) {
@@ -85,8 +107,18 @@ cudaError_t launch_integral2d(const void* img, int dtype, int H, int W, bool squ
     if (square) integral_cols_kernel<double, true><<<blocks, threads, 0, s>>>((const double*)img, H, W, out);
     else integral_cols_kernel<double, false><<<blocks, threads, 0, s>>>((const double*)img, H, W, out);
   }
-  integral_rows_kernel<<<(H + 1 + 127) / 128, 128, 0, s>>>(H, W, out);
+  const int chunks = (W + ICHUNK - 1) / ICHUNK;
+  const dim3 g1((H + 1 + 127) / 128, chunks);
+  integral_rows_chunk_kernel<<<g1, 128, 0, s>>>(H, W, out, scratch);
+  if (chunks > 1) {
+    const dim3 g2((H + 1 + 127) / 128, chunks - 1);
+    integral_rows_offset_kernel<<<g2, 128, 0, s>>>(H, W, out, scratch);
+  }
   return cudaGetLastError();
+}
+
+size_t integral2d_scratch_bytes(int H, int W) {
+  return (size_t)(H + 1) * (size_t)((W + ICHUNK - 1) / ICHUNK + 1) * sizeof(double);
 }
 
 // ---------------------------------------------------------------------------
@@ -154,13 +186,26 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) piv2d_kernel(Piv2dArgs a) {
       sc.meanG = box_sum(a.IIg, a.H, g.g01 + g.lo1, g.g01 + g.hi1, g.g02 + g.lo2, g.g02 + g.hi2) / nG;
     }
 
-    // ---- phase 1: F rows (+ skip test), then G rows; r2c along dim 2 ----
-    constexpr int NJF = (Lay::NF + 31) / 32, NJG = N / 32;
+    // ---- phase 1: F rows and G rows, r2c along dim 2 (one rolled body) ----
+    // The loads of the next row are in flight while the current row is
+    // transformed.
+    constexpr int NJF = (Lay::NF + 31) / 32, NJ = NJF + N / 32;
     double vmax = -INFINITY, sumsq = 0.0;
+    float buf[N];
+    RowJob jn = row_job<N, FPRUNE>(a, g, lane, 0);
+    row_load<N, T>(a, jn, buf);
 #pragma unroll 1
-    for (int job = 0; job < NJF; ++job) {
-      const int row = lane + 32 * job;
-      if (row < Lay::NF) phase1_row<N, FPRUNE, T, ALG == ALG_ZNCC>(a, g, sc, true, row, GH, FH, vmax, sumsq);
+    for (int job = 0; job < NJ; ++job) {
+      const RowJob jc = jn;
+      float cur[N];
+#pragma unroll
+      for (int x = 0; x < N; ++x) cur[x] = buf[x];
+      if (job + 1 < NJ) {
+        jn = row_job<N, FPRUNE>(a, g, lane, job + 1);
+        row_load<N, T>(a, jn, buf);
+      }
+      if (!(jc.isF && jc.row >= Lay::NF))
+        row_process<N, FPRUNE, T, ALG == ALG_ZNCC>(a, sc, jc, cur, GH, FH, vmax, sumsq);
     }
     vmax = warp_max(vmax);
     sc.sumF2 = warp_sum(sumsq);
@@ -179,75 +224,92 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) piv2d_kernel(Piv2dArgs a) {
       __syncwarp();
       continue;
     }
+    __syncwarp();
 #pragma unroll 1
-    for (int job = 0; job < NJG; ++job)
-      phase1_row<N, FPRUNE, T, ALG == ALG_ZNCC>(a, g, sc, false, lane + 32 * job, GH, FH, vmax, sumsq);
+    for (int n = lane; n < M; n += 32) split_G_pair<N, FPRUNE>(GH, tw, n);
     __syncwarp();
 
-    // ---- phase 2: along dim 1 per spectrum row, product, inverse ----
-#pragma unroll 1
-    for (int u = lane; u < M; u += 32) phase2_row<N, FPRUNE>(u, P1, GH, FH);
-    __syncwarp();
-
-    // ---- phase 3: c2r along dim 2 per lag row, similarity -> plane ----
-    // rows [0, lane_rows) one per lane; a short tail of rows (2*SM1+1 just
-    // above 32) is computed by the whole warp, lanes over s2.
+    // ---- phases 2 and 3: one rolled loop of stages around one FFT body ----
+    // rows [0, lane_rows) of phase 3 go one per lane; a short tail of rows
+    // (2*SM1+1 just above 32) is computed by the whole warp afterwards.
+    // The plane is row-contiguous: element (s1, s2) at s1*P2 + s2.
     const int lane_rows = (P1 - 32 > 0 && P1 - 32 <= 4) ? 32 : P1;
+    LagRanges R;
+    R.lo1 = g.tlf1;
+    R.hi1 = 2 * a.SM1 - g.brb1;
+    R.lo2 = g.tlf2;
+    R.hi2 = 2 * a.SM2 - g.brb2;
+    R.shi1 = 2 * a.SM1 - 1 - g.brb1;
+    R.shi2 = 2 * a.SM2 - 1 - g.brb2;
+    PeakAcc acc;
+    acc.best = 0.0;
+    acc.bidx = -1;
+    acc.smax = -INFINITY;
+    acc.ssum = 0.0;
+    {
+      constexpr int RU = (M + 31) / 32;  // spectrum rows per lane
+      const int NS2 = 6 * RU;            // phase-2 stages
+      const int RL = (lane_rows + 31) / 32;
+      float2 t[M];  // carried from the F stage (the product) into the I stage
 #pragma unroll 1
-    for (int s1 = lane; s1 < lane_rows; s1 += 32) {
-      float cc[N];
-      phase3_row<N, FPRUNE>(s1, GH, cc);
+      for (int job = 0; job < NS2 + RL; ++job) {
+        if (job == NS2) __syncwarp();  // all spectra rows finished before phase 3
+        bool active;
+        int st = 0, h = 0, u = 0, s1 = 0;
+        if (job < NS2) {
+          const int q = job % 6;
+          u = lane + 32 * (job / 6);
+          h = q / 3;
+          st = q % 3;
+          active = u < M;
+          if (active) stage_pre<N, FPRUNE>(st, h, GH + u * Lay::GSTR, FH + u * Lay::FSTR, t);
+        } else {
+          s1 = lane + 32 * (job - NS2);
+          active = s1 < lane_rows;
+          if (active) c2r_pre<N, FPRUNE>(s1, GH, t);
+        }
+        if (!active) continue;
+        fft_reg<M, false>(t);
+        if (job < NS2) {
+          stage_post<N, FPRUNE>(st, h, u == 0, P1, GH + u * Lay::GSTR, t);
+        } else {
+          double* prow = plane + s1 * P2;
 #pragma unroll
-      for (int s2 = 0; s2 < N; ++s2)
-        if (s2 < P2) plane[s1 + P1 * s2] = (double)cc[s2] * scale;
-      similarity_row<ALG>(a, g, sc, s1, P1, P2, plane);
+          for (int n = 0; n < M; ++n) {
+            const float2 z = cconj(t[fpos<M>(n)]);
+            if (2 * n < P2) prow[2 * n] = (double)z.x * scale;
+            if (2 * n + 1 < P2) prow[2 * n + 1] = (double)z.y * scale;
+          }
+        }
+      }
     }
+    __syncwarp();
+    // the plane rows are complete only once every lane left phase 3's reads
+#pragma unroll 1
+    for (int s1 = lane; s1 < lane_rows; s1 += 32) finish_row<ALG>(a, g, sc, s1, P1, P2, plane + s1 * P2, R, acc);
 #pragma unroll 1
     for (int s1 = lane_rows; s1 < P1; ++s1)
-      for (int s2 = lane; s2 < P2; s2 += 32)
-        plane[s1 + P1 * s2] =
-            similarity_one<ALG>(a, g, sc, s1, s2, (double)tail_row_value<N, FPRUNE>(GH, tw, s1, s2) * scale);
+      for (int s2 = lane; s2 < P2; s2 += 32) {
+        const double v =
+            finish_one<ALG>(a, g, sc, s1, s2, (double)tail_row_value<N, FPRUNE>(GH, tw, s1, s2) * scale);
+        plane[s1 * P2 + s2] = v;
+        acc_take(acc, R, s1, s2, P1, v);
+      }
     __syncwarp();
-
-    // ---- peak (first_fullovp_peak), SN, Gaussian refinement ----
-    const int lo1 = g.tlf1, hi1 = 2 * a.SM1 - g.brb1;
-    const int lo2 = g.tlf2, hi2 = 2 * a.SM2 - g.brb2;
-    double best = 0.0;
-    int bidx = -1;
-    for (int s1 = lane; s1 < lane_rows && s1 <= hi1; s1 += 32)
-      if (s1 >= lo1) peak_scan_row(plane, P1, s1, lo2, hi2, best, bidx);
-    for (int s1 = lane_rows > lo1 ? lane_rows : lo1; s1 <= hi1; ++s1)
-      for (int s2 = lane; s2 <= hi2; s2 += 32)
-        if (s2 >= lo2) peak_take(plane[s1 + P1 * s2], s1 + P1 * s2, best, bidx);
+    double best = acc.best;
+    int bidx = acc.bidx;
     warp_peak(best, bidx);
     double sn = 0.0;
     if (a.SN) {
       // compute_SN (src/utils/piv_ops.jl:336-367) over [TLF_off, 2SM-1-BRB_off]
-      const int shi1 = 2 * a.SM1 - 1 - g.brb1, shi2 = 2 * a.SM2 - 1 - g.brb2;
-      double smax = -INFINITY, ssum = 0.0;
-      for (int s1 = lane; s1 < lane_rows && s1 <= shi1; s1 += 32) {
-        if (s1 < lo1) continue;
-        for (int s2 = lo2; s2 <= shi2; ++s2) {
-          const double v = plane[s1 + P1 * s2];
-          smax = nmax(smax, v);
-          ssum += v;
-        }
-      }
-      for (int s1 = lane_rows > lo1 ? lane_rows : lo1; s1 <= shi1; ++s1)
-        for (int s2 = lane; s2 <= shi2; s2 += 32) {
-          if (s2 < lo2) continue;
-          const double v = plane[s1 + P1 * s2];
-          smax = nmax(smax, v);
-          ssum += v;
-        }
-      smax = warp_nmax(smax);
-      ssum = warp_sum(ssum);
-      const double len = (double)(shi1 - lo1 + 1) * (double)(shi2 - lo2 + 1);
+      const double smax = warp_nmax(acc.smax);
+      const double ssum = warp_sum(acc.ssum);
+      const double len = (double)(R.shi1 - R.lo1 + 1) * (double)(R.shi2 - R.lo2 + 1);
       sn = smax / ((ssum - smax) / (len - 1.0));
     }
     if (a.planes) {
       double* dst = a.planes + (ia - a.ia_begin) * (long long)P1 * P2;
-      for (int i = lane; i < P1 * P2; i += 32) dst[i] = plane[i];
+      for (int i = lane; i < P1 * P2; i += 32) dst[i] = plane[(i % P1) * P2 + i / P1];
     }
     if (lane == 0) {
       double r1, r2;
@@ -255,7 +317,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) piv2d_kernel(Piv2dArgs a) {
         r1 = -1.0;  // 1-based peak (0, 0): displacement -(SM+1)
         r2 = -1.0;
       } else {
-        refine2d(plane, P1, a.SM1, a.SM2, g, bidx % P1, bidx / P1, best, r1, r2);
+        refine2d(plane, P2, a.SM1, a.SM2, g, bidx % P1, bidx / P1, best, r1, r2);
       }
       a.VF[2 * vfo + 0] = r1 - a.SM1 + d1;
       a.VF[2 * vfo + 1] = r2 - a.SM2 + d2;

@@ -198,137 +198,217 @@ MQP_HD MQP_FI void zero_strided(float2* base, int rows, int stride) {
 // r2c code exists once.  F rows also accumulate the raw max (skip test,
 // src/utils/piv_ops.jl:134-146) and the FP64 sum of squares of the
 // transformed values (sumF2, zncc.jl:131-135, nsqecc.jl:349-353).
+// Phase 1 works through the lane's rows ("jobs": NJF rows of F, then the
+// N/32 rows of G) with the raw loads of the next job in flight while the
+// current one is transformed.  A job's loads read one row of the window
+// along dim 2; lanes are consecutive rows, so each warp load is one
+// coalesced column segment.
+struct RowJob {
+  bool isF;
+  bool live;      // the row holds data (else it is all zero)
+  int row;        // window row (dim 1)
+  int xlo, xhi;   // data columns [xlo, xhi) along dim 2
+  long long base; // image index of (row, column 0)
+};
+
+template <int N, bool FPRUNE>
+MQP_HD MQP_FI RowJob row_job(const Piv2dArgs& a, const IAGeom& g, int lane, int job) {
+  using Lay = Layout2d<N, FPRUNE>;
+  constexpr int NJF = (Lay::NF + 31) / 32;
+  RowJob j;
+  j.isF = job < NJF;
+  j.row = lane + 32 * (j.isF ? job : job - NJF);
+  if (j.isF) {
+    // row y of the interrogation window (copy_inter_region!, src/utils/piv_ops.jl:99-109)
+    j.live = j.row < a.IS1;
+    j.xlo = 0;
+    j.xhi = a.IS2 < (FPRUNE ? N / 2 : N) ? a.IS2 : (FPRUNE ? N / 2 : N);
+    j.base = (long long)(g.ir1 + j.row) + (long long)a.H * g.ir2;
+  } else {
+    // row p of the padded search window: data on the clipped region only
+    // (copy_search_region!, src/utils/piv_ops.jl:115-127)
+    j.live = j.row >= g.lo1 && j.row < g.hi1;
+    j.xlo = g.lo2;
+    j.xhi = g.hi2;
+    j.base = (long long)(g.g01 + j.row) + (long long)a.H * g.g02;
+  }
+  return j;
+}
+
+// raw values of a G job's row (0 outside the data columns).  F rows are read
+// by row_process itself, in the images' own precision.
+template <int N, typename T>
+MQP_HD MQP_FI void row_load(const Piv2dArgs& a, const RowJob& j, float (&v)[N]) {
+  const T* p = reinterpret_cast<const T*>(a.img2) + j.base;
+  const bool live = j.live && !j.isF;
+#pragma unroll
+  for (int x = 0; x < N; ++x)
+    v[x] = (live && x >= j.xlo && x < j.xhi) ? (float)ldg_px<T>(p, (long long)a.H * x) : 0.f;
+}
+
+// Transform one row of phase 1 into its spectra (r2c along dim 2).
+// F rows: the IA row, minus the IA mean for ZNCC (src/utils/zncc_ops.jl:7-12);
+// they accumulate the raw max (skip test, src/utils/piv_ops.jl:134-146) in
+// the images' precision and the FP64 sum of squares of the transformed
+// values (sumF2, zncc.jl:131-135, nsqecc.jl:349-353).  G rows come loaded in
+// v and subtract the search-region mean on their data part for ZNCC
+// (src/utils/zncc_ops.jl:18-25).
 template <int N, bool FPRUNE, typename T, bool ZNCC>
-MQP_HD MQP_FI void phase1_row(const Piv2dArgs& a, const IAGeom& g, const IAScalars& sc, bool isF, int row,
-                              float2* GH, float2* FH, double& vmax, double& sumsq) {
+MQP_HD MQP_FI void row_process(const Piv2dArgs& a, const IAScalars& sc, const RowJob& j, const float (&v)[N],
+                               float2* GH, float2* FH, double& vmax, double& sumsq) {
   using Lay = Layout2d<N, FPRUNE>;
   constexpr int M = N / 2;
-  float2* out = isF ? FH + row : GH + row;
-  const int stride = isF ? Lay::FSTR : Lay::GSTR;
+  float2* out = j.isF ? FH + j.row : GH + j.row;
+  const int stride = j.isF ? Lay::FSTR : Lay::GSTR;
+  if (!j.live) {
+    zero_strided(out, M, stride);
+    return;
+  }
   float2 z[M];
-  if (isF) {
-    if (row >= a.IS1) {
-      zero_strided(out, M, stride);
-      return;
+  if (j.isF) {
+    constexpr int FLIM = FPRUNE ? N / 2 : N;  // columns an IA row can occupy
+    const T* p = reinterpret_cast<const T*>(a.img1) + j.base;
+    T rmax = p[0];
+    float w[N];
+#pragma unroll
+    for (int x = 0; x < N; ++x) {
+      w[x] = 0.f;
+      if (x < FLIM && x < j.xhi) {
+        const T r = ldg_px<T>(p, (long long)a.H * x);
+        rmax = r > rmax ? r : rmax;
+        const double val = (double)r - sc.meanF;
+        sumsq += val * val;
+        w[x] = (float)val;
+      }
     }
-    const long long base = (long long)(g.ir1 + row) + (long long)a.H * g.ir2;
+    vmax = (double)rmax > vmax ? (double)rmax : vmax;
+#pragma unroll
+    for (int n = 0; n < M; ++n) z[n] = make_float2(w[2 * n], w[2 * n + 1]);
+  } else if (ZNCC) {
+    const float mg = (float)sc.meanG;
 #pragma unroll
     for (int n = 0; n < M; ++n) {
-      float v[2];
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int x2 = 2 * n + h;
-        v[h] = 0.f;
-        if ((!FPRUNE || x2 < M) && x2 < a.IS2) {
-          const double r = (double)ldg_px<T>(a.img1, base + (long long)a.H * x2);
-          vmax = r > vmax ? r : vmax;
-          const double val = r - sc.meanF;
-          sumsq += val * val;
-          v[h] = (float)val;
-        }
-      }
-      z[n] = make_float2(v[0], v[1]);
+      const int x0 = 2 * n, x1 = 2 * n + 1;
+      z[n] = make_float2((x0 >= j.xlo && x0 < j.xhi) ? v[x0] - mg : 0.f,
+                         (x1 >= j.xlo && x1 < j.xhi) ? v[x1] - mg : 0.f);
     }
   } else {
-    if (row < g.lo1 || row >= g.hi1) {
-      zero_strided(out, M, stride);
-      return;
-    }
-    const long long base = (long long)(g.g01 + row) + (long long)a.H * g.g02;
-    const float meanG = ZNCC ? (float)sc.meanG : 0.f;
 #pragma unroll
-    for (int n = 0; n < M; ++n) {
-      float v[2];
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int x2 = 2 * n + h;
-        v[h] = 0.f;
-        if (x2 >= g.lo2 && x2 < g.hi2) {
-          const float r = (float)ldg_px<T>(a.img2, base + (long long)a.H * x2);
-          v[h] = ZNCC ? r - meanG : r;
-        }
-      }
-      z[n] = make_float2(v[0], v[1]);
-    }
+    for (int n = 0; n < M; ++n) z[n] = make_float2(v[2 * n], v[2 * n + 1]);
   }
   r2c_store<N, M>(z, out, stride);
 }
 
 // ---------------------------------------------------------------------------
+// after phase 1: first DIF stage along dim 1 for the G spectra
+// ---------------------------------------------------------------------------
+// Splits every G spectrum row u (length N along dim 1) into its even-bin
+// half Ge[n] = g[n] + g[n+N/2] (slots 0..N/2) and odd-bin half
+// Go[n] = (g[n] - g[n+N/2]) W_N^n (slots N/2..N), in place, so phase 2
+// works on half-length transforms.  Lane handles window rows n = lane + 32j.
+// tw: (cos, sin)(2 pi j / N).
+template <int N, bool FPRUNE>
+MQP_HD MQP_FI void split_G_pair(float2* GH, const float2* tw, int n) {
+  using Lay = Layout2d<N, FPRUNE>;
+  constexpr int M = N / 2;
+  const float2 w = tw[n];
+  for (int u = 0; u < M; ++u) {
+    float2* r = GH + u * Lay::GSTR;
+    const float2 a = r[n], b = r[n + M];
+    const float2 d = csub(a, b);
+    r[n] = cadd(a, b);
+    r[n + M] = make_float2(d.x * w.x + d.y * w.y, d.y * w.x - d.x * w.y);  // d * conj(w)
+  }
+}
+
+// ---------------------------------------------------------------------------
 // phase 2: along dim 1 for one spectrum row u (u = 0 is the packed real pair)
 // ---------------------------------------------------------------------------
-// F row u as an N/2-point transform of its even (ODD = 0) or odd (ODD = 1)
-// output bins: F is zero past NF entries, and for the full width the two
-// halves are folded first (the first DIF stage of the N-point transform).
-template <int N, bool FPRUNE, int ODD>
-MQP_HD MQP_FI void load_F_half(const float2* Frow, float2 (&f)[N / 2]) {
-  constexpr int M = N / 2;
-#pragma unroll
-  for (int n = 0; n < M; ++n) {
-    float2 v = Frow[n];
-    if (!FPRUNE) {
-      const float2 w = Frow[n + M];
-      v = ODD ? csub(v, w) : cadd(v, w);
-    }
-    f[n] = ODD ? rotate<N, false>(v, n) : v;
-  }
-  fft_reg<M, false>(f);
-}
-
-// conj(F)*G over the bins k = 2m + ODD of spectrum row u into p (natural
-// order).  Row 0 carries two real rows A + iB (k2 = 0 and k2 = N/2): their
-// spectra are A^ = (Z[k] + conj Z[-k]) / 2 and B^ = -i (Z[k] - conj Z[-k]) / 2,
-// and the two Hermitian products return together as PA + i PB.
-template <int N, int ODD>
-MQP_HD MQP_FI void row_product(bool packed, const float2 (&g)[N], const float2 (&f)[N / 2], float2 (&p)[N]) {
-  constexpr int M = N / 2;
+// conj(F)*G over the N/2 bins k = 2m + h of one half (natural order m).  Row 0
+// carries two real rows A + iB (k2 = 0 and k2 = N/2): their spectra are
+// A^ = (Z[k] + conj Z[-k]) / 2 and B^ = -i (Z[k] - conj Z[-k]) / 2, and the two
+// Hermitian products return together as PA + i PB; the mirror -k of a bin
+// lies in the same half (m' = -m mod N/2 for even bins, N/2-1-m for odd).
+template <int M>
+MQP_HD MQP_FI void half_product(bool packed, int h, const float2 (&x)[M], const float2 (&f)[M], float2 (&p)[M]) {
   if (!packed) {
 #pragma unroll
-    for (int m = 0; m < M; ++m) p[2 * m + ODD] = cmulc(f[fpos<M>(m)], g[fpos<N>(2 * m + ODD)]);
-  } else {
+    for (int m = 0; m < M; ++m) p[m] = cmulc(f[fpos<M>(m)], x[fpos<M>(m)]);
+    return;
+  }
 #pragma unroll
-    for (int m = 0; m < M; ++m) {
-      const int k = 2 * m + ODD;
-      const int nk = (N - k) & (N - 1);
-      if (nk < k) continue;  // written together with its mirror
-      const int nm = nk >> 1;  // the mirror bin has the same parity
-      const float2 Zk = g[fpos<N>(k)], Zn = cconj(g[fpos<N>(nk)]);
-      const float2 Fk = f[fpos<M>(m)], Fn = cconj(f[fpos<M>(nm)]);
-      const float2 A = cscale(cadd(Zk, Zn), 0.5f), B = cscale(cmul_mi(csub(Zk, Zn)), 0.5f);
-      const float2 Af = cscale(cadd(Fk, Fn), 0.5f), Bf = cscale(cmul_mi(csub(Fk, Fn)), 0.5f);
-      const float2 PA = cmulc(Af, A), PB = cmulc(Bf, B);
-      p[k] = cadd(PA, cmul_pi(PB));
-      if (nk != k) p[nk] = cadd(cconj(PA), cmul_pi(cconj(PB)));
+  for (int m = 0; m < M; ++m) {
+    // the mirror of bin 2m+h is 2m'+h with m' = (h ? M-1-m : (M-m) % M)
+    const int me = (M - m) & (M - 1), mo = M - 1 - m;
+    const int mm = h ? mo : me;
+    if (mm < m) continue;  // written together with its mirror
+    const float2 Zk = x[fpos<M>(m)], Zn = cconj(h ? x[fpos<M>(mo)] : x[fpos<M>(me)]);
+    const float2 Fk = f[fpos<M>(m)], Fn = cconj(h ? f[fpos<M>(mo)] : f[fpos<M>(me)]);
+    const float2 A = cscale(cadd(Zk, Zn), 0.5f), B = cscale(cmul_mi(csub(Zk, Zn)), 0.5f);
+    const float2 Af = cscale(cadd(Fk, Fn), 0.5f), Bf = cscale(cmul_mi(csub(Fk, Fn)), 0.5f);
+    const float2 PA = cmulc(Af, A), PB = cmulc(Bf, B);
+    const float2 q = cadd(PA, cmul_pi(PB));
+    const float2 qm = cadd(cconj(PA), cmul_pi(cconj(PB)));
+    if (h) {
+      p[m] = q;
+      if (mo != m) p[mo] = qm;
+    } else {
+      p[m] = q;
+      if (me != m) p[me] = qm;
     }
   }
 }
 
+// One spectrum row: two half passes (even bins, then odd bins) of forward
+// N/2-point transforms of G (already split by split_G_pair) and F, the
+// product, and an N/2-point inverse; the halves recombine as
+//   R[s] = A0[s] + W_N^-s A1[s],  R[s + N/2] = A0[s] - W_N^-s A1[s].
+// The even pass parks A0 in the consumed Ge slots.  Lags s < P1 stay in
+// slots 0..P1 of the row.
 template <int N, bool FPRUNE>
-MQP_HD MQP_FI void phase2_row(int u, int P1, float2* GH, const float2* FH) {
+MQP_HD MQP_FI void phase2_row(int u, int P1, float2* GH, const float2* FH, const float2* tw) {
   using Lay = Layout2d<N, FPRUNE>;
   constexpr int M = N / 2;
   float2* Grow = GH + u * Lay::GSTR;
   const float2* Frow = FH + u * Lay::FSTR;
   const bool packed = (u == 0);
-  float2 g[N];
+#pragma unroll 1
+  for (int h = 0; h < 2; ++h) {
+    float2 x[M];
 #pragma unroll
-  for (int n = 0; n < N; ++n) g[n] = Grow[n];
-  fft_reg<N, false>(g);
-  float2 p[N];
-  {
+    for (int n = 0; n < M; ++n) x[n] = Grow[h * M + n];
+    fft_reg<M, false>(x);
     float2 f[M];
-    load_F_half<N, FPRUNE, 0>(Frow, f);
-    row_product<N, 0>(packed, g, f, p);
-  }
-  {
-    float2 f[M];
-    load_F_half<N, FPRUNE, 1>(Frow, f);
-    row_product<N, 1>(packed, g, f, p);
-  }
-  fft_reg<N, true>(p);
 #pragma unroll
-  for (int s = 0; s < N; ++s)
-    if (s < P1) Grow[s] = p[fpos<N>(s)];
+    for (int n = 0; n < M; ++n) {
+      float2 v = Frow[n];
+      if (!FPRUNE) {
+        const float2 w = Frow[n + M];
+        v = h ? csub(v, w) : cadd(v, w);
+      }
+      f[n] = v;
+    }
+    if (h) {
+#pragma unroll
+      for (int n = 1; n < M; ++n) f[n] = rotate<N, false>(f[n], n);
+    }
+    fft_reg<M, false>(f);
+    float2 p[M];
+    half_product<M>(packed, h, x, f, p);
+    fft_reg<M, true>(p);
+    if (h == 0) {
+#pragma unroll
+      for (int n = 0; n < M; ++n) Grow[n] = p[fpos<M>(n)];
+    } else {
+#pragma unroll
+      for (int n = 0; n < M; ++n) {
+        const float2 a0 = Grow[n];
+        const float2 t = rotate<N, true>(p[fpos<M>(n)], n);
+        if (n < P1) Grow[n] = cadd(a0, t);
+        if (n + M < P1) Grow[n + M] = csub(a0, t);
+      }
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -363,6 +443,141 @@ MQP_HD MQP_FI void phase3_row(int s1, const float2* GH, float (&cc)[N]) {
     const float2 v = x[fpos<M>(n)];
     cc[2 * n] = v.x;
     cc[2 * n + 1] = v.y;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// phases 2 and 3 through one forward FFT body
+// ---------------------------------------------------------------------------
+// Every transform of phases 2 and 3 is an N/2-point complex FFT; running them
+// as the stages of one rolled loop around a single fft_reg call keeps one
+// copy of the transform code in the kernel (the fully unrolled transforms are
+// most of the instruction footprint).  Inverses use
+// IFFT(x) = conj(FFT(conj(x))), the conjugations folded into the
+// neighbouring arithmetic.
+//
+// Stages of one spectrum row (phase 2), h = 0 (even bins) then h = 1:
+//   G : t <- Ge/Go half of the row            -> FFT -> row half <- G^_h
+//   F : t <- F row (folded / twiddled for h)  -> FFT -> t <- conj(conj(F^_h) G^_h)
+//   I : (t holds the conjugated product)      -> FFT -> A_h = conj(t): park (h=0)
+//                                                     or recombine (h=1)
+// and of one lag row (phase 3):
+//   C : t <- conj(E + iO) of the c2r split    -> FFT -> cc = conj(t)
+enum Stage2 : int { ST_G = 0, ST_F = 1, ST_I = 2 };
+
+template <int N, bool FPRUNE>
+MQP_HD MQP_FI void stage_pre(int st, int h, const float2* Grow, const float2* Frow, float2 (&t)[N / 2]) {
+  constexpr int M = N / 2;
+  if (st == ST_G) {
+#pragma unroll
+    for (int n = 0; n < M; ++n) t[n] = Grow[h * M + n];
+  } else if (st == ST_F) {
+#pragma unroll
+    for (int n = 0; n < M; ++n) {
+      float2 v = Frow[n];
+      if (!FPRUNE) {
+        const float2 w = Frow[n + M];
+        v = h ? csub(v, w) : cadd(v, w);
+      }
+      t[n] = v;
+    }
+    if (h) {
+#pragma unroll
+      for (int n = 1; n < M; ++n) t[n] = rotate<N, false>(t[n], n);
+    }
+  }
+}
+
+// conj of the product conj(F^)G^ over one half (natural order m), from the
+// transformed F half in t (fpos slots) and the transformed G half in x
+// (natural order), computed in place in x and then moved to t (keeping two
+// half spectra live, not three); see half_product for the packed row 0.
+template <int M>
+MQP_HD MQP_FI void stage_product(bool packed, int h, float2 (&x)[M], float2 (&t)[M]) {
+  if (!packed) {
+#pragma unroll
+    for (int m = 0; m < M; ++m) x[m] = cconj(cmulc(t[fpos<M>(m)], x[m]));
+  } else {
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      // the mirror of bin 2m+h is 2m'+h with m' = (M-m) % M (h = 0) or M-1-m
+      // (h = 1); h is a runtime value, so both candidates stay compile-time
+      // register indices and a select picks one
+      const int me = (M - m) & (M - 1), mo = M - 1 - m;
+      if (me < m && mo < m) continue;
+      const bool lead = h ? (mo >= m) : (me >= m);  // this m writes the pair
+      const float2 Zk = x[m], Fk = t[fpos<M>(m)];
+      const float2 Zn = cconj(h ? x[mo] : x[me]);
+      const float2 Fn = cconj(h ? t[fpos<M>(mo)] : t[fpos<M>(me)]);
+      const float2 A = cscale(cadd(Zk, Zn), 0.5f), B = cscale(cmul_mi(csub(Zk, Zn)), 0.5f);
+      const float2 Af = cscale(cadd(Fk, Fn), 0.5f), Bf = cscale(cmul_mi(csub(Fk, Fn)), 0.5f);
+      const float2 PA = cmulc(Af, A), PB = cmulc(Bf, B);
+      const float2 qk = cconj(cadd(PA, cmul_pi(PB)));
+      const float2 qn = cconj(cadd(cconj(PA), cmul_pi(cconj(PB))));
+      if (lead) {
+        x[m] = qk;
+        if (h) {
+          if (mo != m) x[mo] = qn;
+        } else {
+          if (me != m) x[me] = qn;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < M; ++m) t[m] = x[m];
+}
+
+template <int N, bool FPRUNE>
+MQP_HD MQP_FI void stage_post(int st, int h, bool packed, int P1, float2* Grow, float2 (&t)[N / 2]) {
+  constexpr int M = N / 2;
+  if (st == ST_G) {
+#pragma unroll
+    for (int n = 0; n < M; ++n) Grow[h * M + n] = t[fpos<M>(n)];
+  } else if (st == ST_F) {
+    float2 x[M];
+#pragma unroll
+    for (int n = 0; n < M; ++n) x[n] = Grow[h * M + n];
+    stage_product<M>(packed, h, x, t);
+  } else {
+    if (h == 0) {
+#pragma unroll
+      for (int n = 0; n < M; ++n) Grow[n] = cconj(t[fpos<M>(n)]);
+    } else {
+#pragma unroll
+      for (int n = 0; n < M; ++n) {
+        const float2 a0 = Grow[n];
+        const float2 r = rotate<N, true>(cconj(t[fpos<M>(n)]), n);
+        if (n < P1) Grow[n] = cadd(a0, r);
+        if (n + M < P1) Grow[n + M] = csub(a0, r);
+      }
+    }
+  }
+}
+
+// phase 3 input: the c2r split of lag column s1 of the spectra rows,
+// conjugated for the inverse through the forward transform
+template <int N, bool FPRUNE>
+MQP_HD MQP_FI void c2r_pre(int s1, const float2* GH, float2 (&t)[N / 2]) {
+  using Lay = Layout2d<N, FPRUNE>;
+  constexpr int M = N / 2;
+  float2 X[M];
+#pragma unroll
+  for (int k = 0; k < M; ++k) X[k] = GH[k * Lay::GSTR + s1];
+  const float X0 = X[0].x, XM = X[0].y;  // the packed real bins X[0], X[N/2]
+#pragma unroll
+  for (int k = 0; k < M; ++k) {
+    float2 E, O;
+    if (k == 0) {
+      E = make_float2(X0 + XM, 0.f);
+      O = make_float2(X0 - XM, 0.f);
+    } else {
+      const float2 A = X[k];
+      const float2 B = cconj(X[M - k]);
+      E = cadd(A, B);
+      O = rotate<N, true>(csub(A, B), k);
+    }
+    t[k] = cconj(cadd(E, cmul_pi(O)));
   }
 }
 
@@ -405,104 +620,9 @@ MQP_HD MQP_FI void lag_window(int s, int IS, int g0, int lo, int hi, int& r0, in
   r1 = g0 + (b > a ? b : a);
 }
 
-// Similarity of lag row s1, in place over plane[s1 + P1*s2] (s2 < P2),
-// which holds the raw correlation c = sum_x F(x) G(x+s):
-//   FFTCC  c                                           (fftcc.jl:123)
-//   ZNCC   c / (sqrt(sum_win G'^2) sqrt(sumF2))        (zncc_ops.jl:29-50)
-//   NSQECC den / (den + num), num = sumF2 + sum_win G^2 - 2c,
-//          den = sqrt(sum_win G^2) sqrt(sumF2)          (nsqecc_ops.jl:1-25)
-// The window sums come from FP64 integral images of img2 / img2^2 (lanes are
-// consecutive lag rows, so each lookup is a coalesced column segment) and
-// the numerator is formed in FP64 (it cancels near a match); the square
-// roots and the final quotient are FP32, whose ~1e-7 relative error is
-// below the FP32 correlation's own.
-template <int ALG>
-MQP_HD MQP_FI void similarity_row(const Piv2dArgs& a, const IAGeom& g, const IAScalars& sc, int s1, int P1,
-                                  int P2, double* plane) {
-  if (ALG == ALG_FFTCC) return;
-  int r0, r1;
-  lag_window(s1, a.IS1, g.g01, g.lo1, g.hi1, r0, r1);
-  const float sqF = sqrtf((float)sc.sumF2);
-  const long long ld = (long long)a.H + 1;
-  const bool rows = r1 > r0;
-  for (int s2 = 0; s2 < P2; ++s2) {
-    int c0, c1;
-    lag_window(s2, a.IS2, g.g02, g.lo2, g.hi2, c0, c1);
-    double S2 = 0.0, S1 = 0.0;
-    if (rows && c1 > c0) {
-      const double* A0 = a.IIg2 + ld * c0;
-      const double* A1 = a.IIg2 + ld * c1;
-      S2 = (A1[r1] - A1[r0]) - (A0[r1] - A0[r0]);
-      if (ALG == ALG_ZNCC) {
-        const double* B0 = a.IIg + ld * c0;
-        const double* B1 = a.IIg + ld * c1;
-        S1 = (B1[r1] - B1[r0]) - (B0[r1] - B0[r0]);
-      }
-    }
-    double& v = plane[s1 + P1 * s2];
-    const double c = v;
-    if (ALG == ALG_NSQECC) {
-      const double num = (sc.sumF2 - 2.0 * c) + S2;
-      const float den = sqrtf((float)S2) * sqF;
-      v = (double)(den / (float)(num + (double)den));
-    } else {
-      const double n = (double)(r1 - r0) * (double)(c1 - c0);
-      double SG = S2 - 2.0 * sc.meanG * S1 + n * sc.meanG * sc.meanG;
-      SG = SG > 0.0 ? SG : 0.0;
-      v = (double)((float)c / (sqrtf((float)SG) * sqF));
-    }
-  }
-}
-
-// similarity_row for one element (s1, s2): the tail rows use it with the
-// lanes spread over s2.
-template <int ALG>
-MQP_HD MQP_FI double similarity_one(const Piv2dArgs& a, const IAGeom& g, const IAScalars& sc, int s1, int s2,
-                                    double c) {
-  if (ALG == ALG_FFTCC) return c;
-  int r0, r1, c0, c1;
-  lag_window(s1, a.IS1, g.g01, g.lo1, g.hi1, r0, r1);
-  lag_window(s2, a.IS2, g.g02, g.lo2, g.hi2, c0, c1);
-  const double S2 = box_sum(a.IIg2, a.H, r0, r1, c0, c1);
-  const float sqF = sqrtf((float)sc.sumF2);
-  if (ALG == ALG_NSQECC) {
-    const double num = (sc.sumF2 - 2.0 * c) + S2;
-    const float den = sqrtf((float)S2) * sqF;
-    return (double)(den / (float)(num + (double)den));
-  }
-  const double S1 = box_sum(a.IIg, a.H, r0, r1, c0, c1);
-  const double n = (double)(r1 - r0) * (double)(c1 - c0);
-  double SG = S2 - 2.0 * sc.meanG * S1 + n * sc.meanG * sc.meanG;
-  SG = SG > 0.0 ? SG : 0.0;
-  return (double)((float)c / (sqrtf((float)SG) * sqF));
-}
-
 // NaN-propagating max / min (Julia's maximum / minimum)
 MQP_HD MQP_FI double nmax(double m, double v) { return (v > m || v != v) ? v : m; }
 MQP_HD MQP_FI double nmin(double m, double v) { return (v < m || v != v) ? v : m; }
-
-// gaussian_refinement + gaussian_2D (src/utils/piv_ops.jl:282-319) around the
-// 0-based peak (p1, p2) of value mx in the P1-row plane; returns the refined
-// 0-based position (unchanged when the peak touches the search range edge).
-MQP_HD MQP_FI void refine2d(const double* plane, int P1, int SM1, int SM2, const IAGeom& g,
-                            int p1, int p2, double mx, double& r1, double& r2) {
-  r1 = p1;
-  r2 = p2;
-  // reference test in 1-based indices: peak > 1 + TLF_off and peak < 1 + 2SM - BRB_off
-  const bool inside = (p1 + 1 > 1 + g.tlf1) && (p2 + 1 > 1 + g.tlf2) &&
-                      (p1 + 1 < 1 + 2 * SM1 - g.brb1) && (p2 + 1 < 1 + 2 * SM2 - g.brb2);
-  if (!inside) return;
-  double mn = plane[(p1 - 1) + P1 * (p2 - 1)];
-  for (int j = -1; j <= 1; ++j)
-    for (int i = -1; i <= 1; ++i) mn = nmin(mn, plane[(p1 + i) + P1 * (p2 + j)]);
-  const double lmx = log(1.0 + mx - mn);
-  const double up = log(1.0 + plane[(p1 - 1) + P1 * p2] - mn);
-  const double down = log(1.0 + plane[(p1 + 1) + P1 * p2] - mn);
-  const double left = log(1.0 + plane[p1 + P1 * (p2 - 1)] - mn);
-  const double right = log(1.0 + plane[p1 + P1 * (p2 + 1)] - mn);
-  r1 = p1 + (up - down) / (2.0 * up - 4.0 * lmx + 2.0 * down);
-  r2 = p2 + (left - right) / (2.0 * left - 4.0 * lmx + 2.0 * right);
-}
 
 // lane-local part of first_fullovp_peak (src/utils/common_ops.jl:98-124).
 // The reference keeps the first maximum > 0 of a column-major scan; every
@@ -510,16 +630,141 @@ MQP_HD MQP_FI void refine2d(const double* plane, int P1, int SM1, int SM2, const
 // it owns, starting from (0, none), and merging lanes by the same rule gives
 // the same element whatever the split.
 MQP_HD MQP_FI void peak_take(double v, int idx, double& best, int& bidx) {
-  // larger value, or the same value earlier in column-major order
   if (v > best || (v == best && idx < bidx)) {
     best = v;
     bidx = idx;
   }
 }
 
-MQP_HD MQP_FI void peak_scan_row(const double* plane, int P1, int s1, int lo2, int hi2, double& best,
-                                 int& bidx) {
-  for (int s2 = lo2; s2 <= hi2; ++s2) peak_take(plane[s1 + P1 * s2], s1 + P1 * s2, best, bidx);
+// Per-lane accumulators of the peak search and of compute_SN
+// (src/utils/piv_ops.jl:336-367), and the 0-based inclusive lag ranges:
+// peak [lo, hi] = [TLF_off, 2SM - BRB_off], SN rows/cols up to 2SM-1-BRB_off.
+struct PeakAcc {
+  double best;
+  int bidx;
+  double smax, ssum;
+};
+struct LagRanges {
+  int lo1, hi1, lo2, hi2, shi1, shi2;
+};
+
+MQP_HD MQP_FI void acc_take(PeakAcc& acc, const LagRanges& R, int s1, int s2, int P1, double v) {
+  if (s1 >= R.lo1 && s2 >= R.lo2) {
+    if (s1 <= R.hi1 && s2 <= R.hi2) peak_take(v, s1 + P1 * s2, acc.best, acc.bidx);
+    if (s1 <= R.shi1 && s2 <= R.shi2) {
+      acc.smax = nmax(acc.smax, v);
+      acc.ssum += v;
+    }
+  }
+}
+
+// Similarity from the raw correlation c and the window sums:
+//   FFTCC  c                                           (fftcc.jl:123)
+//   ZNCC   c / (sqrt(sum_win G'^2) sqrt(sumF2))        (zncc_ops.jl:29-50)
+//   NSQECC den / (den + num), num = sumF2 + sum_win G^2 - 2c,
+//          den = sqrt(sum_win G^2) sqrt(sumF2)          (nsqecc_ops.jl:1-25)
+// The numerator is formed in FP64 (it cancels near a match); the square
+// roots and the final quotient are FP32, whose ~1e-7 relative error is below
+// the FP32 correlation's own.
+template <int ALG>
+MQP_HD MQP_FI double similarity_value(const IAScalars& sc, float sqF, double c, double S2, double S1, double n) {
+  if (ALG == ALG_FFTCC) return c;
+  if (ALG == ALG_NSQECC) {
+    const double num = (sc.sumF2 - 2.0 * c) + S2;
+    const float den = sqrtf((float)S2) * sqF;
+    return (double)(den / (float)(num + (double)den));
+  }
+  double SG = S2 - 2.0 * sc.meanG * S1 + n * sc.meanG * sc.meanG;
+  SG = SG > 0.0 ? SG : 0.0;
+  return (double)((float)c / (sqrtf((float)SG) * sqF));
+}
+
+// Finishes lag row s1: prow[s2] (s2 < P2) holds the raw correlation on entry
+// and the similarity on exit; the row's elements enter the peak / SN
+// accumulators.  Window sums come from the FP64 integral images of img2 and
+// img2^2; lanes are consecutive lag rows, so each lookup is a coalesced
+// column segment, and four lags' lookups are issued before any is used.
+template <int ALG>
+MQP_HD MQP_FI void finish_row(const Piv2dArgs& a, const IAGeom& g, const IAScalars& sc, int s1, int P1,
+                              int P2, double* prow, const LagRanges& R, PeakAcc& acc) {
+  const float sqF = sqrtf((float)sc.sumF2);
+  int r0 = 0, r1 = 0;
+  if (ALG != ALG_FFTCC) lag_window(s1, a.IS1, g.g01, g.lo1, g.hi1, r0, r1);
+  const long long ld = (long long)a.H + 1;
+  for (int b = 0; b < P2; b += 4) {
+    double S2v[4], S1v[4], nv[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      S2v[t] = 0.0;
+      S1v[t] = 0.0;
+      nv[t] = 0.0;
+      const int s2 = b + t;
+      if (ALG != ALG_FFTCC && s2 < P2) {
+        int c0, c1;
+        lag_window(s2, a.IS2, g.g02, g.lo2, g.hi2, c0, c1);
+        if (r1 > r0 && c1 > c0) {
+          const double* A0 = a.IIg2 + ld * c0;
+          const double* A1 = a.IIg2 + ld * c1;
+          S2v[t] = (A1[r1] - A1[r0]) - (A0[r1] - A0[r0]);
+          if (ALG == ALG_ZNCC) {
+            const double* B0 = a.IIg + ld * c0;
+            const double* B1 = a.IIg + ld * c1;
+            S1v[t] = (B1[r1] - B1[r0]) - (B0[r1] - B0[r0]);
+            nv[t] = (double)(r1 - r0) * (double)(c1 - c0);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const int s2 = b + t;
+      if (s2 < P2) {
+        const double v = similarity_value<ALG>(sc, sqF, prow[s2], S2v[t], S1v[t], nv[t]);
+        prow[s2] = v;
+        acc_take(acc, R, s1, s2, P1, v);
+      }
+    }
+  }
+}
+
+// One element (s1, s2) of a tail lag row (the whole warp shares such rows,
+// lanes over s2); c is the raw correlation.
+template <int ALG>
+MQP_HD MQP_FI double finish_one(const Piv2dArgs& a, const IAGeom& g, const IAScalars& sc, int s1, int s2,
+                                double c) {
+  if (ALG == ALG_FFTCC) return c;
+  int r0, r1, c0, c1;
+  lag_window(s1, a.IS1, g.g01, g.lo1, g.hi1, r0, r1);
+  lag_window(s2, a.IS2, g.g02, g.lo2, g.hi2, c0, c1);
+  const double S2 = box_sum(a.IIg2, a.H, r0, r1, c0, c1);
+  const double S1 = ALG == ALG_ZNCC ? box_sum(a.IIg, a.H, r0, r1, c0, c1) : 0.0;
+  const double n = (double)(r1 - r0) * (double)(c1 - c0);
+  return similarity_value<ALG>(sc, sqrtf((float)sc.sumF2), c, S2, S1, n);
+}
+
+// gaussian_refinement + gaussian_2D (src/utils/piv_ops.jl:282-319) around the
+// 0-based peak (p1, p2) of value mx; the plane is row-contiguous (element
+// (s1, s2) at s1*P2 + s2).  Returns the refined 0-based position (unchanged
+// when the peak touches the search range edge).
+MQP_HD MQP_FI void refine2d(const double* plane, int P2, int SM1, int SM2, const IAGeom& g, int p1, int p2,
+                            double mx, double& r1, double& r2) {
+  r1 = p1;
+  r2 = p2;
+  // reference test in 1-based indices: peak > 1 + TLF_off and peak < 1 + 2SM - BRB_off
+  const bool inside = (p1 + 1 > 1 + g.tlf1) && (p2 + 1 > 1 + g.tlf2) &&
+                      (p1 + 1 < 1 + 2 * SM1 - g.brb1) && (p2 + 1 < 1 + 2 * SM2 - g.brb2);
+  if (!inside) return;
+  auto at = [&](int i, int j) { return plane[i * P2 + j]; };
+  double mn = at(p1 - 1, p2 - 1);
+  for (int j = -1; j <= 1; ++j)
+    for (int i = -1; i <= 1; ++i) mn = nmin(mn, at(p1 + i, p2 + j));
+  const double lmx = log(1.0 + mx - mn);
+  const double up = log(1.0 + at(p1 - 1, p2) - mn);
+  const double down = log(1.0 + at(p1 + 1, p2) - mn);
+  const double left = log(1.0 + at(p1, p2 - 1) - mn);
+  const double right = log(1.0 + at(p1, p2 + 1) - mn);
+  r1 = p1 + (up - down) / (2.0 * up - 4.0 * lmx + 2.0 * down);
+  r2 = p2 + (left - right) / (2.0 * left - 4.0 * lmx + 2.0 * right);
 }
 
 // merge two (value, first index) candidates: larger value, then smaller index

@@ -47,8 +47,15 @@ static void emu_ia(const Piv2dArgs& a, long long ia, std::vector<float2>& ws) {
     sc.meanG = box_sum(a.IIg, a.H, g.g01 + g.lo1, g.g01 + g.hi1, g.g02 + g.lo2, g.g02 + g.hi2) / nG;
   }
   double vmax = -INFINITY, sumsq = 0.0;
-  for (int row = 0; row < Lay::NF; ++row)
-    phase1_row<N, FPRUNE, T, ALG == ALG_ZNCC>(a, g, sc, true, row, GH, FH, vmax, sumsq);
+  constexpr int NJF = (Lay::NF + 31) / 32, NJ = NJF + N / 32;
+  for (int lane = 0; lane < 32; ++lane)
+    for (int job = 0; job < NJ; ++job) {
+      const RowJob j = row_job<N, FPRUNE>(a, g, lane, job);
+      if (j.isF && j.row >= Lay::NF) continue;
+      float v[N];
+      row_load<N, T>(a, j, v);
+      row_process<N, FPRUNE, T, ALG == ALG_ZNCC>(a, sc, j, v, GH, FH, vmax, sumsq);
+    }
   sc.sumF2 = sumsq;
   const long long vfo = (long long)v1 + (long long)a.vf1 * v2;
   if (a.threshold >= 0.0 && vmax < a.threshold) {
@@ -58,51 +65,81 @@ static void emu_ia(const Piv2dArgs& a, long long ia, std::vector<float2>& ws) {
     if (a.planes) memset(a.planes + (ia - a.ia_begin) * (long long)P1 * P2, 0, sizeof(double) * P1 * P2);
     return;
   }
-  for (int row = 0; row < N; ++row)
-    phase1_row<N, FPRUNE, T, ALG == ALG_ZNCC>(a, g, sc, false, row, GH, FH, vmax, sumsq);
-  for (int u = 0; u < M; ++u) phase2_row<N, FPRUNE>(u, P1, GH, FH);
-  const double scale = cc_scale<N>();
-  const int lane_rows = (P1 - 32 > 0 && P1 - 32 <= 4) ? 32 : P1;
-  for (int s1 = 0; s1 < lane_rows; ++s1) {
-    float cc[N];
-    phase3_row<N, FPRUNE>(s1, GH, cc);
-    for (int s2 = 0; s2 < P2; ++s2) plane[s1 + P1 * s2] = (double)cc[s2] * scale;
-  }
-  for (int s1 = 0; s1 < lane_rows; ++s1) similarity_row<ALG>(a, g, sc, s1, P1, P2, plane);
   float2 tw[N];
   for (int j = 0; j < N; ++j) tw[j] = twiddle_cs(j * (TW_N / N));
-  for (int s1 = lane_rows; s1 < P1; ++s1)
-    for (int s2 = 0; s2 < P2; ++s2)
-      plane[s1 + P1 * s2] =
-          similarity_one<ALG>(a, g, sc, s1, s2, (double)tail_row_value<N, FPRUNE>(GH, tw, s1, s2) * scale);
-  const int lo1 = g.tlf1, hi1 = 2 * a.SM1 - g.brb1, lo2 = g.tlf2, hi2 = 2 * a.SM2 - g.brb2;
-  double best = 0.0;
+  for (int n = 0; n < M; ++n) split_G_pair<N, FPRUNE>(GH, tw, n);
+  const double scale = cc_scale<N>();
+  const int lane_rows = (P1 - 32 > 0 && P1 - 32 <= 4) ? 32 : P1;
+  // phase 2 stages per spectrum row, then phase 3 rows, as the kernel's loop
+  for (int u = 0; u < M; ++u) {
+    float2 t[M];
+    for (int q = 0; q < 6; ++q) {
+      const int h = q / 3, st = q % 3;
+      stage_pre<N, FPRUNE>(st, h, GH + u * Lay::GSTR, FH + u * Lay::FSTR, t);
+      fft_reg<M, false>(t);
+      stage_post<N, FPRUNE>(st, h, u == 0, P1, GH + u * Lay::GSTR, t);
+    }
+  }
+  for (int s1 = 0; s1 < lane_rows; ++s1) {
+    float2 t[M];
+    c2r_pre<N, FPRUNE>(s1, GH, t);
+    fft_reg<M, false>(t);
+    double* prow = plane + s1 * P2;
+    for (int n = 0; n < M; ++n) {
+      const float2 z = cconj(t[fpos<M>(n)]);
+      if (2 * n < P2) prow[2 * n] = (double)z.x * scale;
+      if (2 * n + 1 < P2) prow[2 * n + 1] = (double)z.y * scale;
+    }
+  }
+  LagRanges R;
+  R.lo1 = g.tlf1;
+  R.hi1 = 2 * a.SM1 - g.brb1;
+  R.lo2 = g.tlf2;
+  R.hi2 = 2 * a.SM2 - g.brb2;
+  R.shi1 = 2 * a.SM1 - 1 - g.brb1;
+  R.shi2 = 2 * a.SM2 - 1 - g.brb2;
+  double best = 0.0, smax = -INFINITY, ssum = 0.0;
   int bidx = -1;
+  // lanes: rows s1 = lane + 32k; tail rows: lanes over s2
   for (int lane = 0; lane < 32; ++lane) {
-    double lb = 0.0;
-    int li = -1;
-    for (int s1 = lane; s1 < lane_rows && s1 <= hi1; s1 += 32)
-      if (s1 >= lo1) peak_scan_row(plane, P1, s1, lo2, hi2, lb, li);
-    for (int s1 = lane_rows > lo1 ? lane_rows : lo1; s1 <= hi1; ++s1)
-      for (int s2 = lane; s2 <= hi2; s2 += 32)
-        if (s2 >= lo2) peak_take(plane[s1 + P1 * s2], s1 + P1 * s2, lb, li);
-    peak_merge(best, bidx, lb, li);
+    PeakAcc acc;
+    acc.best = 0.0;
+    acc.bidx = -1;
+    acc.smax = -INFINITY;
+    acc.ssum = 0.0;
+    for (int s1 = lane; s1 < lane_rows; s1 += 32) finish_row<ALG>(a, g, sc, s1, P1, P2, plane + s1 * P2, R, acc);
+    peak_merge(best, bidx, acc.best, acc.bidx);
+    smax = nmax(smax, acc.smax);
+    ssum += acc.ssum;
+  }
+  for (int lane = 0; lane < 32; ++lane) {
+    PeakAcc acc;
+    acc.best = 0.0;
+    acc.bidx = -1;
+    acc.smax = -INFINITY;
+    acc.ssum = 0.0;
+    for (int s1 = lane_rows; s1 < P1; ++s1)
+      for (int s2 = lane; s2 < P2; s2 += 32) {
+        const double v =
+            finish_one<ALG>(a, g, sc, s1, s2, (double)tail_row_value<N, FPRUNE>(GH, tw, s1, s2) * scale);
+        plane[s1 * P2 + s2] = v;
+        acc_take(acc, R, s1, s2, P1, v);
+      }
+    peak_merge(best, bidx, acc.best, acc.bidx);
+    smax = nmax(smax, acc.smax);
+    ssum += acc.ssum;
   }
   double sn = 0.0;
   if (a.SN) {
-    const int shi1 = 2 * a.SM1 - 1 - g.brb1, shi2 = 2 * a.SM2 - 1 - g.brb2;
-    double smax = -INFINITY, ssum = 0.0;
-    for (int s2 = lo2; s2 <= shi2; ++s2)
-      for (int s1 = lo1; s1 <= shi1; ++s1) {
-        smax = nmax(smax, plane[s1 + P1 * s2]);
-        ssum += plane[s1 + P1 * s2];
-      }
-    const double len = (double)(shi1 - lo1 + 1) * (double)(shi2 - lo2 + 1);
+    const double len = (double)(R.shi1 - R.lo1 + 1) * (double)(R.shi2 - R.lo2 + 1);
     sn = smax / ((ssum - smax) / (len - 1.0));
   }
-  if (a.planes) memcpy(a.planes + (ia - a.ia_begin) * (long long)P1 * P2, plane, sizeof(double) * P1 * P2);
+  if (a.planes) {
+    double* dst = a.planes + (ia - a.ia_begin) * (long long)P1 * P2;
+    for (int i = 0; i < P1 * P2; ++i) dst[i] = plane[(i % P1) * P2 + i / P1];
+  }
   double r1 = -1.0, r2 = -1.0;
-  if (bidx >= 0) refine2d(plane, P1, a.SM1, a.SM2, g, bidx % P1, bidx / P1, best, r1, r2);
+  if (bidx >= 0) refine2d(plane, P2, a.SM1, a.SM2, g, bidx % P1, bidx / P1, best, r1, r2);
   a.VF[2 * vfo] = r1 - a.SM1 + d1;
   a.VF[2 * vfo + 1] = r2 - a.SM2 + d2;
   if (a.SN) a.SN[vfo] = sn;
