@@ -207,8 +207,8 @@ size_t elem_size(int dtype) { return dtype == MQP_F64 ? 8 : 4; }
 
 // Enqueue one pass of the 2D path on device arrays.
 int run_pass_2d(mqp_ctx* ctx, const Problem& pb, const mqp_params* p, const void* d1, const void* d2,
-                int dtype, double* dVF, double* dSN, const int32_t* dpred, double* dplanes,
-                int64_t ia_begin, int64_t ia_end, cudaStream_t s) {
+                const void* dmask, const void* dskip, int dtype, double* dVF, double* dSN,
+                const int32_t* dpred, double* dplanes, int64_t ia_begin, int64_t ia_end, cudaStream_t s) {
   const int H = (int)pb.dims[0], W = (int)pb.dims[1];
   const int SS1 = pb.IS[0] + 2 * pb.SM[0], SS2 = pb.IS[1] + 2 * pb.SM[1];
   if (mqp::piv2d_fft_len(SS1, SS2) == 0)
@@ -220,6 +220,9 @@ int run_pass_2d(mqp_ctx* ctx, const Problem& pb, const mqp_params* p, const void
   memset(&a, 0, sizeof(a));
   a.img1 = d1;
   a.img2 = d2;
+  a.mask = dmask;
+  a.mask_skip = dskip;
+  a.mask_threshold = p->mask_threshold;
   a.dtype = dtype;
   if (pb.alg == mqp::ALG_NSQECC || pb.alg == mqp::ALG_ZNCC) {
     if ((e = ctx->iscratch.ensure(mqp::integral2d_scratch_bytes(H, W))) != cudaSuccess)
@@ -280,8 +283,6 @@ int piv_device_impl(mqp_ctx* ctx, const void* d1, const void* d2, const void* dm
   Problem pb;
   int rc = resolve(ctx, p, ndims, dims, masked, 1, pb);
   if (rc != MQP_OK) return rc;
-  if (masked) return fail(ctx, MQP_ERR_UNSUPPORTED, "masked NSQECC is not available in this build");
-  (void)dmask_skip;
   if (ndims == 3) return fail(ctx, MQP_ERR_UNSUPPORTED, "3D PIV is not available in this build");
   if (pb.n_ia == 0) return MQP_OK;
   if (ia_end < 0) ia_end = pb.n_ia;
@@ -289,7 +290,7 @@ int piv_device_impl(mqp_ctx* ctx, const void* d1, const void* d2, const void* dm
   if (!p->computeSN) dSN = nullptr;
   // multipass without refinement re-runs the scale-1 geometry with identical
   // results (src/multi_quickPIV.jl:57, Q6): one pass gives the same VF/SN
-  return run_pass_2d(ctx, pb, p, d1, d2, dtype, dVF, dSN, nullptr, dplanes, ia_begin, ia_end, s);
+  return run_pass_2d(ctx, pb, p, d1, d2, dmask, dmask_skip, dtype, dVF, dSN, nullptr, dplanes, ia_begin, ia_end, s);
 }
 
 }  // namespace

@@ -159,16 +159,22 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) piv2d_kernel(Piv2dArgs a) {
   extern __shared__ float2 smem[];
   using Lay = Layout2d<N, FPRUNE>;
   constexpr int M = N / 2;
+  constexpr bool MASKED = ALG == ALG_MASK_NSQECC;
   const int P1 = 2 * a.SM1 + 1, P2 = 2 * a.SM2 + 1;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float2* GH = smem + (size_t)warp * Lay::warp_f2(P1, P2);
+  const int wf2 = Lay::warp_f2(P1, P2, MASKED);
+  float2* GH = smem + (size_t)warp * wf2;
   float2* FH = GH + Lay::F_OFF;
   double* plane = reinterpret_cast<double*>(FH);
-  float2* tw = smem + (size_t)WARPS * Lay::warp_f2(P1, P2);  // (cos, sin)(2 pi j / N)
+  float* c1buf = MASKED ? reinterpret_cast<float*>(FH + Lay::region2_f2(P1, P2)) : nullptr;
+  float2* tw = smem + (size_t)WARPS * wf2;  // (cos, sin)(2 pi j / N)
   for (int j = threadIdx.x; j < N; j += blockDim.x) tw[j] = twiddle_cs(j * (TW_N / N));
   __syncthreads();
   const long long nwarps = (long long)gridDim.x * WARPS;
   const double scale = cc_scale<N>();
+  // lag rows [0, lane_rows) go one per lane; a short tail of rows
+  // (2*SM1+1 just above 32) is computed by the whole warp, lanes over s2
+  const int lane_rows = (P1 - 32 > 0 && P1 - 32 <= 4) ? 32 : P1;
 
   for (long long ia = a.ia_begin + (long long)blockIdx.x * WARPS + warp; ia < a.ia_end; ia += nwarps) {
     const int v1 = (int)(ia % a.vf1), v2 = (int)(ia / a.vf1);
@@ -185,33 +191,111 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) piv2d_kernel(Piv2dArgs a) {
       const double nG = (double)(g.hi1 - g.lo1) * (double)(g.hi2 - g.lo2);
       sc.meanG = box_sum(a.IIg, a.H, g.g01 + g.lo1, g.g01 + g.hi1, g.g02 + g.lo2, g.g02 + g.hi2) / nG;
     }
-
-    // ---- phase 1: F rows and G rows, r2c along dim 2 (one rolled body) ----
-    // The loads of the next row are in flight while the current row is
-    // transformed.
-    constexpr int NJF = (Lay::NF + 31) / 32, NJ = NJF + N / 32;
-    double vmax = -INFINITY, sumsq = 0.0;
-    float buf[N];
-    RowJob jn = row_job<N, FPRUNE>(a, g, lane, 0);
-    row_load<N, T>(a, jn, buf);
-#pragma unroll 1
-    for (int job = 0; job < NJ; ++job) {
-      const RowJob jc = jn;
-      float cur[N];
-#pragma unroll
-      for (int x = 0; x < N; ++x) cur[x] = buf[x];
-      if (job + 1 < NJ) {
-        jn = row_job<N, FPRUNE>(a, g, lane, job + 1);
-        row_load<N, T>(a, jn, buf);
-      }
-      if (!(jc.isF && jc.row >= Lay::NF))
-        row_process<N, FPRUNE, T, ALG == ALG_ZNCC>(a, sc, jc, cur, GH, FH, vmax, sumsq);
-    }
-    vmax = warp_max(vmax);
-    sc.sumF2 = warp_sum(sumsq);
     const long long vfo = (long long)v1 + (long long)a.vf1 * v2;
-    if (a.threshold >= 0.0 && vmax < a.threshold) {
-      // skip_inter_region (src/utils/piv_ops.jl:140-146): the vector stays zero
+    bool skipped = false;
+
+    // One pass correlates one pair of inputs; masked NSQECC needs two
+    // ((F*mask) with G, mask with G^2, mask_nsqecc.jl:151-155).
+    constexpr int NPASS = MASKED ? 2 : 1;
+#pragma unroll 1
+    for (int pass = 0; pass < NPASS; ++pass) {
+      const int pmode = MASKED ? (pass == 0 ? PASS_MASKED : PASS_MASK_SQ) : PASS_PLAIN;
+
+      // ---- phase 1: F rows and G rows, r2c along dim 2 (one rolled body) ----
+      // The loads of the next row are in flight while the current row is
+      // transformed.
+      constexpr int NJF = (Lay::NF + 31) / 32, NJ = NJF + N / 32;
+      double vmax = -INFINITY, mmax = -INFINITY, sumsq = 0.0;
+      float buf[N];
+      RowJob jn = row_job<N, FPRUNE>(a, g, lane, 0);
+      row_load<N, T>(a, jn, buf);
+#pragma unroll 1
+      for (int job = 0; job < NJ; ++job) {
+        const RowJob jc = jn;
+        float cur[N];
+#pragma unroll
+        for (int x = 0; x < N; ++x) cur[x] = buf[x];
+        if (job + 1 < NJ) {
+          jn = row_job<N, FPRUNE>(a, g, lane, job + 1);
+          row_load<N, T>(a, jn, buf);
+        }
+        if (!(jc.isF && jc.row >= Lay::NF))
+          row_process<N, FPRUNE, T, ALG == ALG_ZNCC>(a, sc, pmode, jc, cur, GH, FH, vmax, mmax, sumsq);
+      }
+      if (pass == 0) {
+        vmax = warp_max(vmax);
+        sc.sumF2 = warp_sum(sumsq);
+        // skip_inter_region (src/utils/piv_ops.jl:134-157): the vector stays zero
+        bool skip;
+        if (MASKED) {
+          mmax = warp_max(mmax);
+          skip = (a.threshold > 0.0 && vmax < a.threshold) || (a.mask_threshold > 0.0 && mmax < a.mask_threshold);
+        } else {
+          skip = a.threshold >= 0.0 && vmax < a.threshold;
+        }
+        if (skip) {
+          skipped = true;
+          break;
+        }
+      }
+      __syncwarp();
+#pragma unroll 1
+      for (int n = lane; n < M; n += 32) split_G_pair<N, FPRUNE>(GH, tw, n);
+      __syncwarp();
+
+      // ---- phases 2 and 3: one rolled loop of stages around one FFT body ----
+      // The plane is row-contiguous: element (s1, s2) at s1*P2 + s2.
+      {
+        constexpr int RU = (M + 31) / 32;  // spectrum rows per lane
+        const int NS2 = 6 * RU;            // phase-2 stages
+        const int RL = (lane_rows + 31) / 32;
+        float2 t[M];  // carried from the F stage (the product) into the I stage
+#pragma unroll 1
+        for (int job = 0; job < NS2 + RL; ++job) {
+          if (job == NS2) __syncwarp();  // all spectra rows finished before phase 3
+          bool active;
+          int st = 0, h = 0, u = 0, s1 = 0;
+          if (job < NS2) {
+            const int q = job % 6;
+            u = lane + 32 * (job / 6);
+            h = q / 3;
+            st = q % 3;
+            active = u < M;
+            if (active) stage_pre<N, FPRUNE>(st, h, GH + u * Lay::GSTR, FH + u * Lay::FSTR, t);
+          } else {
+            s1 = lane + 32 * (job - NS2);
+            active = s1 < lane_rows;
+            if (active) c2r_pre<N, FPRUNE>(s1, GH, t);
+          }
+          if (!active) continue;
+          fft_reg<M, false>(t);
+          if (job < NS2) {
+            stage_post<N, FPRUNE>(st, h, u == 0, P1, GH + u * Lay::GSTR, t);
+          } else {
+            double* prow = plane + s1 * P2;
+#pragma unroll
+            for (int n = 0; n < M; ++n) {
+              const float2 z = cconj(t[fpos<M>(n)]);
+              if (2 * n < P2) prow[2 * n] = (double)z.x * scale;
+              if (2 * n + 1 < P2) prow[2 * n + 1] = (double)z.y * scale;
+            }
+          }
+        }
+      }
+      __syncwarp();
+      // raw correlation of the tail lag rows, all lanes over s2
+#pragma unroll 1
+      for (int s1 = lane_rows; s1 < P1; ++s1)
+        for (int s2 = lane; s2 < P2; s2 += 32)
+          plane[s1 * P2 + s2] = (double)tail_row_value<N, FPRUNE>(GH, tw, s1, s2) * scale;
+      __syncwarp();
+      if (MASKED && pass == 0) {
+        // park (F*mask)*G while the second pass reuses the workspace
+        for (int i = lane; i < P1 * P2; i += 32) c1buf[i] = (float)plane[i];
+        __syncwarp();
+      }
+    }
+    if (skipped) {
       if (lane == 0) {
         a.VF[2 * vfo + 0] = 0.0;
         a.VF[2 * vfo + 1] = 0.0;
@@ -224,16 +308,8 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) piv2d_kernel(Piv2dArgs a) {
       __syncwarp();
       continue;
     }
-    __syncwarp();
-#pragma unroll 1
-    for (int n = lane; n < M; n += 32) split_G_pair<N, FPRUNE>(GH, tw, n);
-    __syncwarp();
 
-    // ---- phases 2 and 3: one rolled loop of stages around one FFT body ----
-    // rows [0, lane_rows) of phase 3 go one per lane; a short tail of rows
-    // (2*SM1+1 just above 32) is computed by the whole warp afterwards.
-    // The plane is row-contiguous: element (s1, s2) at s1*P2 + s2.
-    const int lane_rows = (P1 - 32 > 0 && P1 - 32 <= 4) ? 32 : P1;
+    // ---- finish: similarity, peak (first_fullovp_peak), SN, Gaussian fit ----
     LagRanges R;
     R.lo1 = g.tlf1;
     R.hi1 = 2 * a.SM1 - g.brb1;
@@ -246,54 +322,15 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) piv2d_kernel(Piv2dArgs a) {
     acc.bidx = -1;
     acc.smax = -INFINITY;
     acc.ssum = 0.0;
-    {
-      constexpr int RU = (M + 31) / 32;  // spectrum rows per lane
-      const int NS2 = 6 * RU;            // phase-2 stages
-      const int RL = (lane_rows + 31) / 32;
-      float2 t[M];  // carried from the F stage (the product) into the I stage
 #pragma unroll 1
-      for (int job = 0; job < NS2 + RL; ++job) {
-        if (job == NS2) __syncwarp();  // all spectra rows finished before phase 3
-        bool active;
-        int st = 0, h = 0, u = 0, s1 = 0;
-        if (job < NS2) {
-          const int q = job % 6;
-          u = lane + 32 * (job / 6);
-          h = q / 3;
-          st = q % 3;
-          active = u < M;
-          if (active) stage_pre<N, FPRUNE>(st, h, GH + u * Lay::GSTR, FH + u * Lay::FSTR, t);
-        } else {
-          s1 = lane + 32 * (job - NS2);
-          active = s1 < lane_rows;
-          if (active) c2r_pre<N, FPRUNE>(s1, GH, t);
-        }
-        if (!active) continue;
-        fft_reg<M, false>(t);
-        if (job < NS2) {
-          stage_post<N, FPRUNE>(st, h, u == 0, P1, GH + u * Lay::GSTR, t);
-        } else {
-          double* prow = plane + s1 * P2;
-#pragma unroll
-          for (int n = 0; n < M; ++n) {
-            const float2 z = cconj(t[fpos<M>(n)]);
-            if (2 * n < P2) prow[2 * n] = (double)z.x * scale;
-            if (2 * n + 1 < P2) prow[2 * n + 1] = (double)z.y * scale;
-          }
-        }
-      }
-    }
-    __syncwarp();
-    // the plane rows are complete only once every lane left phase 3's reads
-#pragma unroll 1
-    for (int s1 = lane; s1 < lane_rows; s1 += 32) finish_row<ALG>(a, g, sc, s1, P1, P2, plane + s1 * P2, R, acc);
+    for (int s1 = lane; s1 < lane_rows; s1 += 32)
+      finish_row<ALG>(a, g, sc, s1, P1, P2, plane + s1 * P2, R, acc, MASKED ? c1buf + s1 * P2 : nullptr);
 #pragma unroll 1
     for (int s1 = lane_rows; s1 < P1; ++s1)
       for (int s2 = lane; s2 < P2; s2 += 32) {
-        const double v =
-            finish_one<ALG>(a, g, sc, s1, s2, (double)tail_row_value<N, FPRUNE>(GH, tw, s1, s2) * scale);
-        plane[s1 * P2 + s2] = v;
-        acc_take(acc, R, s1, s2, P1, v);
+        double& e = plane[s1 * P2 + s2];
+        e = finish_one<ALG>(a, g, sc, s1, s2, e, MASKED ? (double)c1buf[s1 * P2 + s2] : 0.0);
+        acc_take(acc, R, s1, s2, P1, e);
       }
     __syncwarp();
     double best = acc.best;
@@ -347,7 +384,7 @@ template <int N, bool FPRUNE, int ALG, typename T, int WARPS, int MINB>
 static cudaError_t launch_t(const Piv2dArgs& a, cudaStream_t s, std::string& err) {
   using Lay = Layout2d<N, FPRUNE>;
   const int P1 = 2 * a.SM1 + 1, P2 = 2 * a.SM2 + 1;
-  const size_t smem = ((size_t)WARPS * Lay::warp_f2(P1, P2) + N) * sizeof(float2);
+  const size_t smem = ((size_t)WARPS * Lay::warp_f2(P1, P2, ALG == ALG_MASK_NSQECC) + N) * sizeof(float2);
   auto kern = piv2d_kernel<N, FPRUNE, ALG, T, WARPS, MINB>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) {
@@ -379,6 +416,8 @@ static cudaError_t launch_alg(const Piv2dArgs& a, int alg, cudaStream_t s, std::
     case ALG_FFTCC: return launch_t<N, FPRUNE, ALG_FFTCC, T, WARPS, MINB>(a, s, err);
     case ALG_ZNCC: return launch_t<N, FPRUNE, ALG_ZNCC, T, WARPS, MINB>(a, s, err);
     case ALG_NSQECC: return launch_t<N, FPRUNE, ALG_NSQECC, T, WARPS, MINB>(a, s, err);
+    // 29.7 KB per warp: three warps per block keep two blocks per SM
+    case ALG_MASK_NSQECC: return launch_t<N, FPRUNE, ALG_MASK_NSQECC, T, 3, MINB>(a, s, err);
     default: err = "unknown correlation algorithm"; return cudaErrorInvalidValue;
   }
 }

@@ -40,7 +40,8 @@ struct Piv2dArgs {
   const void* img1;
   const void* img2;
   const void* mask;      // masked NSQECC interrogation-area mask (or null)
-  int dtype;             // 0 = float32 images, 1 = float64 images
+  const void* mask_skip; // masked NSQECC skip mask (the double-masked method), or null = mask
+  int dtype;             // 0 = float32 images, 1 = float64 images (masks share it)
   const double* II1;     // integral of img1 (ZNCC mean of F), (H+1)x(W+1)
   const double* IIg;     // integral of img2 (ZNCC)
   const double* IIg2;    // integral of img2^2 (ZNCC, NSQECC)
@@ -52,7 +53,8 @@ struct Piv2dArgs {
   int IS1, IS2, SM1, SM2, st1, st2;
   int vf1, vf2;
   long long ia_begin, ia_end;  // IA linear index range processed by this launch
-  double threshold;      // skip when max(IA) < threshold (threshold >= 0)
+  double threshold;      // skip when max(IA) < threshold (threshold >= 0; masked: > 0)
+  double mask_threshold; // masked: skip when max(mask_skip IA) < mask_threshold (> 0)
   int computeSN;
   int* status;           // device error flag (non-zero = failure), or null
 };
@@ -149,7 +151,11 @@ struct Layout2d {
   static MQP_HD MQP_FI int region2_f2(int P1, int P2) {
     return F_SIZE > P1 * P2 ? F_SIZE : P1 * P2;   // one double == one float2
   }
-  static MQP_HD MQP_FI int warp_f2(int P1, int P2) { return G_SIZE + region2_f2(P1, P2); }
+  // masked NSQECC parks its first correlation (FP32, P1 x P2) after the plane
+  static MQP_HD MQP_FI int extra_f2(bool masked, int P1, int P2) { return masked ? (P1 * P2 + 1) / 2 : 0; }
+  static MQP_HD MQP_FI int warp_f2(int P1, int P2, bool masked = false) {
+    return G_SIZE + region2_f2(P1, P2) + extra_f2(masked, P1, P2);
+  }
 };
 
 // ---------------------------------------------------------------------------
@@ -246,16 +252,29 @@ MQP_HD MQP_FI void row_load(const Piv2dArgs& a, const RowJob& j, float (&v)[N]) 
     v[x] = (live && x >= j.xlo && x < j.xhi) ? (float)ldg_px<T>(p, (long long)a.H * x) : 0.f;
 }
 
+// Which inputs a phase-1 pass correlates.
+enum Pass1 : int {
+  PASS_PLAIN = 0,   // F (minus mean for ZNCC) with G (minus mean for ZNCC)
+  PASS_MASKED = 1,  // masked NSQECC, first correlation: F*mask with G
+  PASS_MASK_SQ = 2  // masked NSQECC, second correlation: mask with G^2
+};
+
 // Transform one row of phase 1 into its spectra (r2c along dim 2).
-// F rows: the IA row, minus the IA mean for ZNCC (src/utils/zncc_ops.jl:7-12);
-// they accumulate the raw max (skip test, src/utils/piv_ops.jl:134-146) in
-// the images' precision and the FP64 sum of squares of the transformed
-// values (sumF2, zncc.jl:131-135, nsqecc.jl:349-353).  G rows come loaded in
-// v and subtract the search-region mean on their data part for ZNCC
-// (src/utils/zncc_ops.jl:18-25).
+// F rows: the IA row (copy_inter_region!, src/utils/piv_ops.jl:99-109), minus
+// the IA mean for ZNCC (src/utils/zncc_ops.jl:7-12), times the mask for
+// masked NSQECC (copy_inter_masked!, src/utils/masked_nsqecc_ops.jl:19-25) or
+// the mask itself for its second correlation; they accumulate the raw
+// maxima of the skip tests (src/utils/piv_ops.jl:134-157) in the images'
+// precision and the FP64 sum of squares of the transformed values (sumF2:
+// zncc.jl:131-135, nsqecc.jl:349-353; masked sum(maskF^2/wi),
+// mask_nsqecc.jl:141-149).  G rows come loaded in v and subtract the
+// search-region mean on their data part for ZNCC (src/utils/zncc_ops.jl:18-25),
+// or are squared for the masked second correlation (copy_search_squared!,
+// src/utils/masked_nsqecc_ops.jl:35-42).
 template <int N, bool FPRUNE, typename T, bool ZNCC>
-MQP_HD MQP_FI void row_process(const Piv2dArgs& a, const IAScalars& sc, const RowJob& j, const float (&v)[N],
-                               float2* GH, float2* FH, double& vmax, double& sumsq) {
+MQP_HD MQP_FI void row_process(const Piv2dArgs& a, const IAScalars& sc, int PASS, const RowJob& j,
+                               const float (&v)[N], float2* GH, float2* FH, double& vmax, double& mmax,
+                               double& sumsq) {
   using Lay = Layout2d<N, FPRUNE>;
   constexpr int M = N / 2;
   float2* out = j.isF ? FH + j.row : GH + j.row;
@@ -268,20 +287,34 @@ MQP_HD MQP_FI void row_process(const Piv2dArgs& a, const IAScalars& sc, const Ro
   if (j.isF) {
     constexpr int FLIM = FPRUNE ? N / 2 : N;  // columns an IA row can occupy
     const T* p = reinterpret_cast<const T*>(a.img1) + j.base;
-    T rmax = p[0];
+    const T* q = PASS != PASS_PLAIN ? reinterpret_cast<const T*>(a.mask) + j.base : p;
+    const T* qs = PASS == PASS_MASKED ? reinterpret_cast<const T*>(a.mask_skip ? a.mask_skip : a.mask) + j.base : p;
     float w[N];
 #pragma unroll
     for (int x = 0; x < N; ++x) {
       w[x] = 0.f;
       if (x < FLIM && x < j.xhi) {
-        const T r = ldg_px<T>(p, (long long)a.H * x);
-        rmax = r > rmax ? r : rmax;
-        const double val = (double)r - sc.meanF;
-        sumsq += val * val;
-        w[x] = (float)val;
+        const long long off = (long long)a.H * x;
+        if (PASS == PASS_PLAIN) {
+          const T r = ldg_px<T>(p, off);
+          vmax = (double)r > vmax ? (double)r : vmax;
+          const double val = (double)r - sc.meanF;
+          sumsq += val * val;
+          w[x] = (float)val;
+        } else if (PASS == PASS_MASKED) {
+          const T r = ldg_px<T>(p, off);
+          const T mk = ldg_px<T>(q, off);
+          const T ms = ldg_px<T>(qs, off);
+          vmax = (double)r > vmax ? (double)r : vmax;
+          mmax = (double)ms > mmax ? (double)ms : mmax;
+          const double val = (double)r * (double)mk;
+          sumsq += val * val / ((double)mk > 0.0 ? (double)mk : 1.0);
+          w[x] = (float)val;
+        } else {
+          w[x] = (float)ldg_px<T>(q, off);
+        }
       }
     }
-    vmax = (double)rmax > vmax ? (double)rmax : vmax;
 #pragma unroll
     for (int n = 0; n < M; ++n) z[n] = make_float2(w[2 * n], w[2 * n + 1]);
   } else if (ZNCC) {
@@ -292,6 +325,9 @@ MQP_HD MQP_FI void row_process(const Piv2dArgs& a, const IAScalars& sc, const Ro
       z[n] = make_float2((x0 >= j.xlo && x0 < j.xhi) ? v[x0] - mg : 0.f,
                          (x1 >= j.xlo && x1 < j.xhi) ? v[x1] - mg : 0.f);
     }
+  } else if (PASS == PASS_MASK_SQ) {
+#pragma unroll
+    for (int n = 0; n < M; ++n) z[n] = make_float2(v[2 * n] * v[2 * n], v[2 * n + 1] * v[2 * n + 1]);
   } else {
 #pragma unroll
     for (int n = 0; n < M; ++n) z[n] = make_float2(v[2 * n], v[2 * n + 1]);
@@ -669,6 +705,13 @@ MQP_HD MQP_FI void acc_take(PeakAcc& acc, const LagRanges& R, int s1, int s2, in
 template <int ALG>
 MQP_HD MQP_FI double similarity_value(const IAScalars& sc, float sqF, double c, double S2, double S1, double n) {
   if (ALG == ALG_FFTCC) return c;
+  if (ALG == ALG_MASK_NSQECC) {
+    // fftcc2masknsqecc! (src/utils/masked_nsqecc_ops.jl:123-142): c = (F*mask)*G,
+    // S2 = mask*G^2, both correlations
+    const double num = (sc.sumF2 - 2.0 * c) + S2;
+    const float den = sqrtf(fabsf((float)S2)) * sqF;
+    return (double)(den / (float)(num + (double)den));
+  }
   if (ALG == ALG_NSQECC) {
     const double num = (sc.sumF2 - 2.0 * c) + S2;
     const float den = sqrtf((float)S2) * sqF;
@@ -686,8 +729,17 @@ MQP_HD MQP_FI double similarity_value(const IAScalars& sc, float sqF, double c, 
 // column segment, and four lags' lookups are issued before any is used.
 template <int ALG>
 MQP_HD MQP_FI void finish_row(const Piv2dArgs& a, const IAGeom& g, const IAScalars& sc, int s1, int P1,
-                              int P2, double* prow, const LagRanges& R, PeakAcc& acc) {
+                              int P2, double* prow, const LagRanges& R, PeakAcc& acc, const float* c1row = nullptr) {
   const float sqF = sqrtf((float)sc.sumF2);
+  if (ALG == ALG_MASK_NSQECC) {
+    // prow holds mask*G^2, c1row the parked (F*mask)*G
+    for (int s2 = 0; s2 < P2; ++s2) {
+      const double v = similarity_value<ALG>(sc, sqF, (double)c1row[s2], prow[s2], 0.0, 0.0);
+      prow[s2] = v;
+      acc_take(acc, R, s1, s2, P1, v);
+    }
+    return;
+  }
   int r0 = 0, r1 = 0;
   if (ALG != ALG_FFTCC) lag_window(s1, a.IS1, g.g01, g.lo1, g.hi1, r0, r1);
   const long long ld = (long long)a.H + 1;
@@ -731,8 +783,10 @@ MQP_HD MQP_FI void finish_row(const Piv2dArgs& a, const IAGeom& g, const IAScala
 // lanes over s2); c is the raw correlation.
 template <int ALG>
 MQP_HD MQP_FI double finish_one(const Piv2dArgs& a, const IAGeom& g, const IAScalars& sc, int s1, int s2,
-                                double c) {
+                                double c, double cmask = 0.0) {
   if (ALG == ALG_FFTCC) return c;
+  // masked: c = mask*G^2, cmask = (F*mask)*G
+  if (ALG == ALG_MASK_NSQECC) return similarity_value<ALG>(sc, sqrtf((float)sc.sumF2), cmask, c, 0.0, 0.0);
   int r0, r1, c0, c1;
   lag_window(s1, a.IS1, g.g01, g.lo1, g.hi1, r0, r1);
   lag_window(s2, a.IS2, g.g02, g.lo2, g.hi2, c0, c1);

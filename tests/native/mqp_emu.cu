@@ -31,10 +31,16 @@ template <int N, bool FPRUNE, int ALG, typename T>
 static void emu_ia(const Piv2dArgs& a, long long ia, std::vector<float2>& ws) {
   using Lay = Layout2d<N, FPRUNE>;
   constexpr int M = N / 2;
+  constexpr bool MASKED = ALG == ALG_MASK_NSQECC;
   const int P1 = 2 * a.SM1 + 1, P2 = 2 * a.SM2 + 1;
   float2* GH = ws.data();
   float2* FH = GH + Lay::F_OFF;
   double* plane = reinterpret_cast<double*>(FH);
+  float* c1buf = MASKED ? reinterpret_cast<float*>(FH + Lay::region2_f2(P1, P2)) : nullptr;
+  float2 tw[N];
+  for (int j = 0; j < N; ++j) tw[j] = twiddle_cs(j * (TW_N / N));
+  const double scale = cc_scale<N>();
+  const int lane_rows = (P1 - 32 > 0 && P1 - 32 <= 4) ? 32 : P1;
   const int v1 = (int)(ia % a.vf1), v2 = (int)(ia / a.vf1);
   int d1, d2;
   ia_pred(a, v1, v2, d1, d2);
@@ -46,50 +52,58 @@ static void emu_ia(const Piv2dArgs& a, long long ia, std::vector<float2>& ws) {
     const double nG = (double)(g.hi1 - g.lo1) * (double)(g.hi2 - g.lo2);
     sc.meanG = box_sum(a.IIg, a.H, g.g01 + g.lo1, g.g01 + g.hi1, g.g02 + g.lo2, g.g02 + g.hi2) / nG;
   }
-  double vmax = -INFINITY, sumsq = 0.0;
-  constexpr int NJF = (Lay::NF + 31) / 32, NJ = NJF + N / 32;
-  for (int lane = 0; lane < 32; ++lane)
-    for (int job = 0; job < NJ; ++job) {
-      const RowJob j = row_job<N, FPRUNE>(a, g, lane, job);
-      if (j.isF && j.row >= Lay::NF) continue;
-      float v[N];
-      row_load<N, T>(a, j, v);
-      row_process<N, FPRUNE, T, ALG == ALG_ZNCC>(a, sc, j, v, GH, FH, vmax, sumsq);
-    }
-  sc.sumF2 = sumsq;
   const long long vfo = (long long)v1 + (long long)a.vf1 * v2;
-  if (a.threshold >= 0.0 && vmax < a.threshold) {
-    a.VF[2 * vfo] = 0.0;
-    a.VF[2 * vfo + 1] = 0.0;
-    if (a.SN) a.SN[vfo] = 0.0;
-    if (a.planes) memset(a.planes + (ia - a.ia_begin) * (long long)P1 * P2, 0, sizeof(double) * P1 * P2);
-    return;
-  }
-  float2 tw[N];
-  for (int j = 0; j < N; ++j) tw[j] = twiddle_cs(j * (TW_N / N));
-  for (int n = 0; n < M; ++n) split_G_pair<N, FPRUNE>(GH, tw, n);
-  const double scale = cc_scale<N>();
-  const int lane_rows = (P1 - 32 > 0 && P1 - 32 <= 4) ? 32 : P1;
-  // phase 2 stages per spectrum row, then phase 3 rows, as the kernel's loop
-  for (int u = 0; u < M; ++u) {
-    float2 t[M];
-    for (int q = 0; q < 6; ++q) {
-      const int h = q / 3, st = q % 3;
-      stage_pre<N, FPRUNE>(st, h, GH + u * Lay::GSTR, FH + u * Lay::FSTR, t);
+  constexpr int NPASS = MASKED ? 2 : 1;
+  for (int pass = 0; pass < NPASS; ++pass) {
+    const int pmode = MASKED ? (pass == 0 ? PASS_MASKED : PASS_MASK_SQ) : PASS_PLAIN;
+    double vmax = -INFINITY, mmax = -INFINITY, sumsq = 0.0;
+    constexpr int NJF = (Lay::NF + 31) / 32, NJ = NJF + N / 32;
+    for (int lane = 0; lane < 32; ++lane)
+      for (int job = 0; job < NJ; ++job) {
+        const RowJob j = row_job<N, FPRUNE>(a, g, lane, job);
+        if (j.isF && j.row >= Lay::NF) continue;
+        float v[N];
+        row_load<N, T>(a, j, v);
+        row_process<N, FPRUNE, T, ALG == ALG_ZNCC>(a, sc, pmode, j, v, GH, FH, vmax, mmax, sumsq);
+      }
+    if (pass == 0) {
+      sc.sumF2 = sumsq;
+      const bool skip = MASKED ? ((a.threshold > 0.0 && vmax < a.threshold) ||
+                                  (a.mask_threshold > 0.0 && mmax < a.mask_threshold))
+                               : (a.threshold >= 0.0 && vmax < a.threshold);
+      if (skip) {
+        a.VF[2 * vfo] = 0.0;
+        a.VF[2 * vfo + 1] = 0.0;
+        if (a.SN) a.SN[vfo] = 0.0;
+        if (a.planes) memset(a.planes + (ia - a.ia_begin) * (long long)P1 * P2, 0, sizeof(double) * P1 * P2);
+        return;
+      }
+    }
+    for (int n = 0; n < M; ++n) split_G_pair<N, FPRUNE>(GH, tw, n);
+    for (int u = 0; u < M; ++u) {
+      float2 t[M];
+      for (int q = 0; q < 6; ++q) {
+        const int h = q / 3, st = q % 3;
+        stage_pre<N, FPRUNE>(st, h, GH + u * Lay::GSTR, FH + u * Lay::FSTR, t);
+        fft_reg<M, false>(t);
+        stage_post<N, FPRUNE>(st, h, u == 0, P1, GH + u * Lay::GSTR, t);
+      }
+    }
+    for (int s1 = 0; s1 < lane_rows; ++s1) {
+      float2 t[M];
+      c2r_pre<N, FPRUNE>(s1, GH, t);
       fft_reg<M, false>(t);
-      stage_post<N, FPRUNE>(st, h, u == 0, P1, GH + u * Lay::GSTR, t);
+      double* prow = plane + s1 * P2;
+      for (int n = 0; n < M; ++n) {
+        const float2 z = cconj(t[fpos<M>(n)]);
+        if (2 * n < P2) prow[2 * n] = (double)z.x * scale;
+        if (2 * n + 1 < P2) prow[2 * n + 1] = (double)z.y * scale;
+      }
     }
-  }
-  for (int s1 = 0; s1 < lane_rows; ++s1) {
-    float2 t[M];
-    c2r_pre<N, FPRUNE>(s1, GH, t);
-    fft_reg<M, false>(t);
-    double* prow = plane + s1 * P2;
-    for (int n = 0; n < M; ++n) {
-      const float2 z = cconj(t[fpos<M>(n)]);
-      if (2 * n < P2) prow[2 * n] = (double)z.x * scale;
-      if (2 * n + 1 < P2) prow[2 * n + 1] = (double)z.y * scale;
-    }
+    for (int s1 = lane_rows; s1 < P1; ++s1)
+      for (int s2 = 0; s2 < P2; ++s2) plane[s1 * P2 + s2] = (double)tail_row_value<N, FPRUNE>(GH, tw, s1, s2) * scale;
+    if (MASKED && pass == 0)
+      for (int i = 0; i < P1 * P2; ++i) c1buf[i] = (float)plane[i];
   }
   LagRanges R;
   R.lo1 = g.tlf1;
@@ -100,30 +114,19 @@ static void emu_ia(const Piv2dArgs& a, long long ia, std::vector<float2>& ws) {
   R.shi2 = 2 * a.SM2 - 1 - g.brb2;
   double best = 0.0, smax = -INFINITY, ssum = 0.0;
   int bidx = -1;
-  // lanes: rows s1 = lane + 32k; tail rows: lanes over s2
   for (int lane = 0; lane < 32; ++lane) {
     PeakAcc acc;
     acc.best = 0.0;
     acc.bidx = -1;
     acc.smax = -INFINITY;
     acc.ssum = 0.0;
-    for (int s1 = lane; s1 < lane_rows; s1 += 32) finish_row<ALG>(a, g, sc, s1, P1, P2, plane + s1 * P2, R, acc);
-    peak_merge(best, bidx, acc.best, acc.bidx);
-    smax = nmax(smax, acc.smax);
-    ssum += acc.ssum;
-  }
-  for (int lane = 0; lane < 32; ++lane) {
-    PeakAcc acc;
-    acc.best = 0.0;
-    acc.bidx = -1;
-    acc.smax = -INFINITY;
-    acc.ssum = 0.0;
+    for (int s1 = lane; s1 < lane_rows; s1 += 32)
+      finish_row<ALG>(a, g, sc, s1, P1, P2, plane + s1 * P2, R, acc, MASKED ? c1buf + s1 * P2 : nullptr);
     for (int s1 = lane_rows; s1 < P1; ++s1)
       for (int s2 = lane; s2 < P2; s2 += 32) {
-        const double v =
-            finish_one<ALG>(a, g, sc, s1, s2, (double)tail_row_value<N, FPRUNE>(GH, tw, s1, s2) * scale);
-        plane[s1 * P2 + s2] = v;
-        acc_take(acc, R, s1, s2, P1, v);
+        double& e = plane[s1 * P2 + s2];
+        e = finish_one<ALG>(a, g, sc, s1, s2, e, MASKED ? (double)c1buf[s1 * P2 + s2] : 0.0);
+        acc_take(acc, R, s1, s2, P1, e);
       }
     peak_merge(best, bidx, acc.best, acc.bidx);
     smax = nmax(smax, acc.smax);
@@ -148,7 +151,7 @@ static void emu_ia(const Piv2dArgs& a, long long ia, std::vector<float2>& ws) {
 template <int N, bool FPRUNE, int ALG>
 static void emu_run(const Piv2dArgs& a) {
   using Lay = Layout2d<N, FPRUNE>;
-  std::vector<float2> ws((size_t)Lay::warp_f2(2 * a.SM1 + 1, 2 * a.SM2 + 1));
+  std::vector<float2> ws((size_t)Lay::warp_f2(2 * a.SM1 + 1, 2 * a.SM2 + 1, ALG == ALG_MASK_NSQECC));
   for (long long ia = a.ia_begin; ia < a.ia_end; ++ia) {
     if (a.dtype == 0) emu_ia<N, FPRUNE, ALG, float>(a, ia, ws);
     else emu_ia<N, FPRUNE, ALG, double>(a, ia, ws);
@@ -160,19 +163,23 @@ static int emu_alg(const Piv2dArgs& a, int alg) {
   if (alg == 0) emu_run<N, FPRUNE, 0>(a);
   else if (alg == 1) emu_run<N, FPRUNE, 1>(a);
   else if (alg == 2) emu_run<N, FPRUNE, 2>(a);
+  else if (alg == 3) emu_run<N, FPRUNE, 3>(a);
   else return -1;
   return 0;
 }
 
 extern "C" __attribute__((visibility("default"))) int mqp_emu_piv2d(
-    const void* img1, const void* img2, int dtype, int H, int W, int IS1, int IS2, int SM1, int SM2,
-    int st1, int st2, int alg, double threshold, int computeSN, double* VF, double* SN, double* planes,
-    long long ia_begin, long long ia_end) {
+    const void* img1, const void* img2, const void* mask, const void* mask_skip, int dtype, int H, int W,
+    int IS1, int IS2, int SM1, int SM2, int st1, int st2, int alg, double threshold, double mask_threshold,
+    int computeSN, double* VF, double* SN, double* planes, long long ia_begin, long long ia_end) {
   std::vector<double> II1, IIg, IIg2;
   Piv2dArgs a;
   memset(&a, 0, sizeof(a));
   a.img1 = img1;
   a.img2 = img2;
+  a.mask = mask;
+  a.mask_skip = mask_skip;
+  a.mask_threshold = mask_threshold;
   a.dtype = dtype;
   if (alg == 1 || alg == 2) {
     integral(img2, dtype, H, W, true, IIg2);

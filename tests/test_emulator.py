@@ -8,7 +8,7 @@ import pytest
 
 import oracle.piv_oracle as O
 from multi_quickpiv_b200 import synth
-from tests.helpers import PLANE_RTOL, VF_ATOL, compare_planes, sn_ok
+from tests.helpers import MASK_PLANE_RTOL, PLANE_RTOL, VF_ATOL, compare_planes, mask_coverage, sn_ok
 from tests.native import build_emu
 
 ALG = {"fft": 0, "zncc": 1, "nsqecc": 2}
@@ -31,7 +31,7 @@ def test_register_fft(emu, n):
         assert np.max(np.abs(y - ref)) / np.max(np.abs(ref)) < 3e-7
 
 
-def run_emu(emu, i1, i2, alg, IS, SM, st, thr=-1.0):
+def run_emu(emu, i1, i2, alg, IS, SM, st, thr=-1.0, mask=None, mask_skip=None, mthr=-1.0):
     vf = O.get_vectorfield_size(i1.shape, IS, st)
     n = vf[0] * vf[1]
     P1, P2 = 2 * SM[0] + 1, 2 * SM[1] + 1
@@ -40,9 +40,13 @@ def run_emu(emu, i1, i2, alg, IS, SM, st, thr=-1.0):
     PL = np.zeros((P1, P2, n), order="F")
     dt = 1 if i1.dtype == np.float64 else 0
     f1, f2 = np.asfortranarray(i1), np.asfortranarray(i2)
-    p = lambda a: a.ctypes.data_as(C.c_void_p)
-    rc = emu.mqp_emu_piv2d(p(f1), p(f2), dt, i1.shape[0], i1.shape[1], IS[0], IS[1], SM[0], SM[1], st[0], st[1],
-                           ALG[alg], C.c_double(thr), 1, p(VF), p(SN), p(PL), C.c_longlong(0), C.c_longlong(n))
+    fm = np.asfortranarray(mask, dtype=i1.dtype) if mask is not None else None
+    fs = np.asfortranarray(mask_skip, dtype=i1.dtype) if mask_skip is not None else None
+    p = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)
+    code = 3 if mask is not None else ALG[alg]
+    rc = emu.mqp_emu_piv2d(p(f1), p(f2), p(fm), p(fs), dt, i1.shape[0], i1.shape[1], IS[0], IS[1], SM[0], SM[1],
+                           st[0], st[1], code, C.c_double(thr), C.c_double(mthr), 1, p(VF), p(SN), p(PL),
+                           C.c_longlong(0), C.c_longlong(n))
     assert rc == 0
     return VF, SN, PL
 
@@ -73,3 +77,39 @@ def test_emulated_threshold_skip(emu):
     i1[:40, :40] = -10.0
     VF, SN, _ = run_emu(emu, i1, i2, "fft", (32, 32), (16, 16), (16, 16), thr=0.0)
     assert np.all(VF[:, 0, 0] == 0) and SN[0, 0] == 0
+
+
+@pytest.mark.parametrize("cfg", [((32, 32), (16, 16), (16, 16)), ((16, 16), (8, 8), (8, 8)),
+                                 ((24, 32), (12, 8), (12, 10))])
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_emulated_masked_nsqecc(emu, cfg, dtype):
+    IS, SM, st = cfg
+    i1, i2, _ = synth.pair_2d_shift(shape=(112, 100), seed_stream=22)
+    i1, i2 = i1.astype(dtype), i2.astype(dtype)
+    mask = synth.ellipse_mask(np.random.default_rng(7), i1.shape, cover=0.7).astype(dtype)
+    po = O.set_piv_parameters(interSize=IS, searchMargin=SM, step=st, computeSN=True)
+    po.ndims = 2
+    VFo, SNo, Co = O.piv_single_pass(i1, i2, po, mask=mask, keep_corr=True)
+    VF, SN, PL = run_emu(emu, i1, i2, "nsqecc", IS, SM, st, mask=mask)
+    # masked sums of a nearly empty mask sit at the FP32 FFT noise floor (it
+    # scales with the whole window); planes are compared where the mask covers
+    # at least a quarter of the IA, displacements everywhere
+    sparse = mask_coverage(mask, i1.shape, IS, st) < 0.25
+    worst, near_tie = compare_planes(PL, Co, i1.shape, IS, SM, st, skip=sparse)
+    assert worst <= MASK_PLANE_RTOL, worst
+    bad = (np.abs(VF - VFo) > VF_ATOL).any(axis=0) & ~near_tie
+    assert not bad.any(), np.abs(VF - VFo).max()
+
+
+def test_emulated_masked_skip(emu):
+    i1, i2, _ = synth.pair_2d_shift(shape=(96, 96))
+    mask = np.ones_like(i1)
+    skipm = np.ones_like(i1)
+    skipm[:40, :40] = 0.0
+    po = O.set_piv_parameters(interSize=(32, 32), searchMargin=(16, 16), step=(16, 16), computeSN=True,
+                              mask_threshold=0.5)
+    po.ndims = 2
+    VFo, SNo = O.piv_single_pass(i1, i2, po, mask=mask, mask_skip=skipm)
+    VF, SN, _ = run_emu(emu, i1, i2, "nsqecc", (32, 32), (16, 16), (16, 16), mask=mask, mask_skip=skipm, mthr=0.5)
+    assert np.all(VF[:, 0, 0] == 0) and np.all(VFo[:, 0, 0] == 0)
+    assert np.max(np.abs(VF - VFo)) < 1e-3

@@ -5,7 +5,7 @@ import pytest
 
 import oracle.piv_oracle as O
 from multi_quickpiv_b200 import PIV, correlation_planes, setPIVParameters, synth
-from tests.helpers import PLANE_RTOL, VF_ATOL, compare_planes, sn_ok
+from tests.helpers import MASK_PLANE_RTOL, PLANE_RTOL, VF_ATOL, compare_planes, mask_coverage, sn_ok
 
 pytestmark = pytest.mark.gpu
 
@@ -69,3 +69,45 @@ def test_float32_precision_output(gpu):
     pp = setPIVParameters(corr_alg="fft", interSize=(32, 32), searchMargin=(16, 16), step=(16, 16))
     VF, SN = PIV(i1, i2, pp, precision=np.float32)
     assert VF.dtype == np.float32 and SN is None
+
+
+@pytest.mark.parametrize("cfg", [((32, 32), (16, 16), (16, 16)), ((16, 16), (8, 8), (8, 8)),
+                                 ((24, 32), (12, 8), (12, 10))])
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_masked_nsqecc_matches_oracle(cfg, dtype, gpu):
+    """PIV(img1, img2, mask, pivparams) (src/multi_quickPIV.jl:22-24): masked
+    NSQECC with an ellipse mask, against the oracle's restatement of
+    _mask_NSQECC! (src/crosscorrelation_algorithms/mask_nsqecc.jl:126-160)."""
+    IS, SM, st = cfg
+    i1, i2, _ = synth.pair_2d_shift(shape=(128, 112), seed_stream=23)
+    i1, i2 = i1.astype(dtype), i2.astype(dtype)
+    mask = synth.ellipse_mask(np.random.default_rng(8), i1.shape, cover=0.7).astype(dtype)
+    po = _oracle_params("nsqecc", IS, SM, st)
+    VFo, SNo, Co = O.piv_single_pass(i1, i2, po, mask=mask, keep_corr=True)
+    pp = setPIVParameters(interSize=IS, searchMargin=SM, step=st, computeSN=True)
+    VF, SN = PIV(i1, i2, mask, pp)
+    planes = correlation_planes(i1, i2, pp, mask=mask)
+    sparse = mask_coverage(mask, i1.shape, IS, st) < 0.25
+    worst, near_tie = compare_planes(planes, Co, i1.shape, IS, SM, st, skip=sparse)
+    assert worst <= MASK_PLANE_RTOL, worst
+    bad = (np.abs(VF - VFo) > VF_ATOL).any(axis=0) & ~near_tie
+    assert not bad.any(), np.nanmax(np.abs(VF - VFo))
+
+
+def test_double_masked_skip(gpu):
+    """PIV(img1, img2, mask_VF, mask_IA, pivparams) (src/multi_quickPIV.jl:27-29):
+    the first mask drives the skip test (mask_threshold > 0), the second the
+    correlation."""
+    i1, i2, _ = synth.pair_2d_shift(shape=(96, 96), seed_stream=24)
+    mask_ia = np.ones_like(i1)
+    mask_vf = np.ones_like(i1)
+    mask_vf[:40, :40] = 0.0
+    pp = setPIVParameters(interSize=(32, 32), searchMargin=(16, 16), step=(16, 16), computeSN=True,
+                          mask_threshold=0.5)
+    VF, SN = PIV(i1, i2, mask_vf, mask_ia, pp)
+    po = O.set_piv_parameters(interSize=(32, 32), searchMargin=(16, 16), step=(16, 16), computeSN=True,
+                              mask_threshold=0.5)
+    po.ndims = 2
+    VFo, SNo = O.piv_single_pass(i1, i2, po, mask=mask_ia, mask_skip=mask_vf)
+    assert np.all(VF[:, 0, 0] == 0) and np.all(VFo[:, 0, 0] == 0)
+    assert np.nanmax(np.abs(VF - VFo)) < VF_ATOL
