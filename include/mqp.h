@@ -151,6 +151,39 @@ typedef struct mqp_profile {
 MQP_API int mqp_profile_enable(mqp_ctx* ctx, int enable); /* also resets the counters */
 MQP_API int mqp_profile_read(mqp_ctx* ctx, mqp_profile* out);
 
+/*
+ * Allocation-free 2D PIV.  No counterpart in the reference: it exists for
+ * callers that cannot allocate GPU memory when they compute a vector field
+ * (code running under a framework that owns all device memory through its
+ * own pool, real-time loops that must not meet cudaMalloc's implicit
+ * synchronisation or failure mid-run, hosts that budget every device byte
+ * up front).  It computes what mqp_piv_device computes for 2D images
+ * (FFTCC, ZNCC, NSQECC; no mask) on caller-owned device arrays, without a
+ * context and without allocating: its only scratch is a fixed array of
+ * MQP_NOALLOC_SCRATCH_BYTES built into the library, which every GPU that
+ * loads the library holds until the process exits.
+ *
+ *  - Scratch needed: NSQECC one, ZNCC three FP64 integral images of
+ *    (dims[0]+1) x (dims[1]+1) doubles plus about 1/8 of one for scan totals;
+ *    FFTCC none.  48 MiB covers NSQECC up to about 2400 x 2400 and ZNCC up to
+ *    about 1400 x 1400.  Larger images are rejected with MQP_ERR_INVALID and
+ *    a message; use mqp_piv_device for them.
+ *  - The first call on a device looks up the scratch array's device address
+ *    (with that device current) and caches it; make that first call before
+ *    any stream capture.
+ *  - All calls share the one scratch array and it keeps the last call's
+ *    contents (every element is rewritten before it is read, so nothing needs
+ *    clearing).  Calls whose GPU work overlaps (different streams, or
+ *    different host threads on one device) race on it: serialise them.
+ *  - Work is enqueued on `stream` (NULL = the legacy default stream); errors
+ *    are written to err (errlen bytes, may be NULL) and returned as MQP_ERR_*.
+ */
+#define MQP_NOALLOC_SCRATCH_BYTES (48u * 1024u * 1024u)
+
+MQP_API int mqp_piv2d_noalloc(const void* d_img1, const void* d_img2, int dtype, const int64_t dims[2],
+                              const mqp_params* p, double* d_VF, double* d_SN, void* stream, char* err,
+                              int errlen);
+
 #ifdef __cplusplus
 }
 #endif

@@ -73,6 +73,8 @@ SIGNATURES = {
                                  I64x3, C.POINTER(MqpParams), C.c_void_p, C.c_void_p, C.c_void_p]),
     "mqp_correlation_planes": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
                                          I64x3, C.POINTER(MqpParams), C.c_int64, C.c_int64, C.c_void_p]),
+    "mqp_piv2d_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int64 * 2, C.POINTER(MqpParams),
+                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, C.c_int]),
     "mqp_profile_enable": (C.c_int, [C.c_void_p, C.c_int]),
     "mqp_profile_read": (C.c_int, [C.c_void_p, C.POINTER(MqpProfile)]),
 }
