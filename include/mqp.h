@@ -151,6 +151,15 @@ typedef struct mqp_profile {
 MQP_API int mqp_profile_enable(mqp_ctx* ctx, int enable); /* also resets the counters */
 MQP_API int mqp_profile_read(mqp_ctx* ctx, mqp_profile* out);
 
+/* Launch tuning of a context (no counterpart in the reference, whose FFTW
+ * plans take no such knobs).  Results never depend on these values.
+ *   MQP_TUNE_CHUNK3D         IAs per chunk of the 3D path (0 = from the budget)
+ *   MQP_TUNE_CHUNK3D_BUDGET  device bytes of 3D chunk scratch (default 1 GiB)
+ * Returns MQP_ERR_INVALID for an unknown key or a negative value. */
+#define MQP_TUNE_CHUNK3D 1
+#define MQP_TUNE_CHUNK3D_BUDGET 2
+MQP_API int mqp_set_tuning(mqp_ctx* ctx, int key, int64_t value);
+
 /*
  * Allocation-free 2D PIV.  No counterpart in the reference: it exists for
  * callers that cannot allocate GPU memory when they compute a vector field

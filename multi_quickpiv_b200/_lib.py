@@ -22,6 +22,7 @@ MQP_ERR_BUSY = -6
 MQP_ERR_NOT_FOUND = -7
 
 MQP_FFTCC, MQP_ZNCC, MQP_NSQECC, MQP_MASK_NSQECC = 0, 1, 2, 3
+MQP_TUNE_CHUNK3D, MQP_TUNE_CHUNK3D_BUDGET = 1, 2
 MQP_F32, MQP_F64 = 0, 1
 
 # every symbol declared in include/mqp.h, with its ctypes signature
@@ -77,6 +78,7 @@ SIGNATURES = {
                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, C.c_int]),
     "mqp_profile_enable": (C.c_int, [C.c_void_p, C.c_int]),
     "mqp_profile_read": (C.c_int, [C.c_void_p, C.POINTER(MqpProfile)]),
+    "mqp_set_tuning": (C.c_int, [C.c_void_p, C.c_int, C.c_int64]),
 }
 
 _lib = None
@@ -131,6 +133,11 @@ class Context:
         out = MqpProfile()
         check(self.lib.mqp_profile_read(self.handle, C.byref(out)), self.handle)
         return {f: getattr(out, f) for f, _ in MqpProfile._fields_}
+
+    def set_chunk3d(self, ias: int = 0, budget_bytes: int = 0):
+        """IAs per 3D chunk (0: as many as budget_bytes of scratch hold)."""
+        check(self.lib.mqp_set_tuning(self.handle, MQP_TUNE_CHUNK3D, int(ias)), self.handle)
+        check(self.lib.mqp_set_tuning(self.handle, MQP_TUNE_CHUNK3D_BUDGET, int(budget_bytes)), self.handle)
 
     def close(self):
         if getattr(self, "handle", None):

@@ -43,7 +43,11 @@ struct mqp_ctx {
   cudaStream_t stream = nullptr;
   std::string last_error;
   std::mutex mu;
-  DevBuf img1, img2, mask, mask_skip, II1, IIg, IIg2, VF, SN, pred, planes, status, iscratch;
+  DevBuf img1, img2, mask, mask_skip, II1, IIg, IIg2, VF, SN, pred, planes, status, iscratch, scratch3d;
+  DevBuf passVF[2];  // vectors of the coarse passes of a multi-pass refinement
+  // 3D path: IAs per chunk (0 = sized from chunk3d_budget bytes of scratch)
+  int64_t chunk3d = 0;
+  size_t chunk3d_budget = (size_t)1 << 30;
   // tracing
   bool profile = false;
   struct Span {
@@ -176,7 +180,8 @@ int mqp_destroy(mqp_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (DevBuf* b : {&ctx->img1, &ctx->img2, &ctx->mask, &ctx->mask_skip, &ctx->II1, &ctx->IIg, &ctx->IIg2,
-                    &ctx->VF, &ctx->SN, &ctx->pred, &ctx->planes, &ctx->status, &ctx->iscratch})
+                    &ctx->VF, &ctx->SN, &ctx->pred, &ctx->planes, &ctx->status, &ctx->iscratch,
+                    &ctx->scratch3d, &ctx->passVF[0], &ctx->passVF[1]})
     b->release();
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -274,6 +279,163 @@ int run_pass_2d(mqp_ctx* ctx, const Problem& pb, const mqp_params* p, const void
   return MQP_OK;
 }
 
+size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
+
+// Enqueue one pass of the 3D path on device arrays.
+int run_pass_3d(mqp_ctx* ctx, const Problem& pb, const mqp_params* p, const void* d1, const void* d2,
+                const void* dmask, const void* dskip, int dtype, double* dVF, double* dSN,
+                const int32_t* dpred, double* dplanes, int64_t ia_begin, int64_t ia_end, cudaStream_t s) {
+  const int H = (int)pb.dims[0], W = (int)pb.dims[1], D = (int)pb.dims[2];
+  const int SS[3] = {pb.IS[0] + 2 * pb.SM[0], pb.IS[1] + 2 * pb.SM[1], pb.IS[2] + 2 * pb.SM[2]};
+  if (mqp::piv3d_fft_len(SS) == 0)
+    return fail(ctx, MQP_ERR_UNSUPPORTED, "3D search window (interSize + 2 searchMargin) above 64 is not supported yet");
+  if (ia_end <= ia_begin) return MQP_OK;
+  cudaError_t e;
+  mqp::Piv3dArgs a;
+  memset(&a, 0, sizeof(a));
+  const bool need_g2 = pb.alg == mqp::ALG_NSQECC || pb.alg == mqp::ALG_ZNCC;
+  const bool need_g1 = pb.alg == mqp::ALG_ZNCC;
+  const size_t ii_bytes = (size_t)(H + 1) * (size_t)(W + 1) * (size_t)(D + 1) * sizeof(double);
+  if (need_g2) {
+    if ((e = ctx->iscratch.ensure(mqp::integral3d_scratch_bytes(H, W, D))) != cudaSuccess)
+      return cuda_fail(ctx, e, "integral scratch");
+    double* isc = (double*)ctx->iscratch.ptr;
+    ProfileScope ps(ctx, s, 0, 0);
+    if ((e = ctx->IIg2.ensure(ii_bytes)) != cudaSuccess) return cuda_fail(ctx, e, "integral buffer");
+    if ((e = mqp::launch_integral3d(d2, dtype, H, W, D, true, (double*)ctx->IIg2.ptr, isc, s)) != cudaSuccess)
+      return cuda_fail(ctx, e, "integral volume of img2^2");
+    a.IIg2 = (const double*)ctx->IIg2.ptr;
+    if (need_g1) {
+      if ((e = ctx->IIg.ensure(ii_bytes)) != cudaSuccess) return cuda_fail(ctx, e, "integral buffer");
+      if ((e = ctx->II1.ensure(ii_bytes)) != cudaSuccess) return cuda_fail(ctx, e, "integral buffer");
+      if ((e = mqp::launch_integral3d(d2, dtype, H, W, D, false, (double*)ctx->IIg.ptr, isc, s)) != cudaSuccess)
+        return cuda_fail(ctx, e, "integral volume of img2");
+      if ((e = mqp::launch_integral3d(d1, dtype, H, W, D, false, (double*)ctx->II1.ptr, isc, s)) != cudaSuccess)
+        return cuda_fail(ctx, e, "integral volume of img1");
+      a.IIg = (const double*)ctx->IIg.ptr;
+      a.II1 = (const double*)ctx->II1.ptr;
+    }
+  }
+  // chunk scratch: Gz | Fz | C | C2 | V | state, each 256-byte aligned
+  const size_t per_ia = mqp::piv3d_scratch_bytes_per_ia(pb.IS, pb.SM, pb.alg);
+  const int64_t n = ia_end - ia_begin;
+  int64_t chunk = ctx->chunk3d > 0 ? ctx->chunk3d : (int64_t)(ctx->chunk3d_budget / per_ia);
+  if (chunk < 1) chunk = 1;
+  if (chunk > 65535) chunk = 65535;
+  if (chunk > n) chunk = n;
+  const int N = mqp::piv3d_fft_len(SS);
+  const bool prune = pb.IS[0] <= N / 2 && pb.IS[1] <= N / 2 && pb.IS[2] <= N / 2;
+  const size_t K3 = N / 2 + 1, NF = prune ? N / 2 : N;
+  const size_t P12 = (size_t)(2 * pb.SM[0] + 1) * (2 * pb.SM[1] + 1), P3 = 2 * pb.SM[2] + 1;
+  const size_t c = (size_t)chunk;
+  const size_t bGz = align256(c * K3 * N * N * sizeof(float2));
+  const size_t bFz = align256(c * K3 * NF * NF * sizeof(float2));
+  const size_t bC = align256(c * K3 * P12 * sizeof(float2));
+  const size_t bC2 = pb.alg == mqp::ALG_MASK_NSQECC ? bC : 0;
+  const size_t bV = align256(c * P12 * P3 * sizeof(float));
+  const size_t bS = align256(c * sizeof(mqp::IA3State));
+  if ((e = ctx->scratch3d.ensure(bGz + bFz + bC + bC2 + bV + bS)) != cudaSuccess) return cuda_fail(ctx, e, "3D scratch");
+  char* base = (char*)ctx->scratch3d.ptr;
+  a.Gz = (float2*)base;
+  a.Fz = (float2*)(base + bGz);
+  a.C = (float2*)(base + bGz + bFz);
+  a.C2 = bC2 ? (float2*)(base + bGz + bFz + bC) : nullptr;
+  a.V = (float*)(base + bGz + bFz + bC + bC2);
+  a.state = (mqp::IA3State*)(base + bGz + bFz + bC + bC2 + bV);
+  a.img1 = d1;
+  a.img2 = d2;
+  a.mask = dmask;
+  a.mask_skip = dskip;
+  a.dtype = dtype;
+  a.pred = dpred;
+  a.VF = dVF;
+  a.SN = dSN;
+  a.planes = dplanes;
+  a.planes_begin = ia_begin;
+  a.H = H;
+  a.W = W;
+  a.D = D;
+  for (int d = 0; d < 3; ++d) {
+    a.IS[d] = pb.IS[d];
+    a.SM[d] = pb.SM[d];
+    a.st[d] = pb.st[d];
+    a.vf[d] = (int)pb.vf[d];
+  }
+  a.ia_begin = ia_begin;
+  a.ia_end = ia_end;
+  a.threshold = p->threshold;
+  a.mask_threshold = p->mask_threshold;
+  std::string err;
+  {
+    ProfileScope ps(ctx, s, 1, ia_end - ia_begin);
+    e = mqp::launch_piv3d(a, pb.alg, chunk, s, err);
+  }
+  if (e != cudaSuccess) return fail(ctx, e == cudaErrorInvalidValue ? MQP_ERR_UNSUPPORTED : MQP_ERR_CUDA, err);
+  return MQP_OK;
+}
+
+// Multi-pass refinement (mqp_params.refine): passes at scales 2^(m-1), ..., 1,
+// each after the first searching around the whole-pixel predictor taken from
+// the previous pass (mqp_multipass.cuh).  SN and the debug planes come from
+// the final pass only, as the reference's compute_SN runs at scale 1.
+int run_multipass(mqp_ctx* ctx, const mqp_params* p, const void* d1, const void* d2, const void* dmask,
+                  const void* dskip, int dtype, int ndims, const int64_t dims[3], double* dVF, double* dSN,
+                  cudaStream_t s, double* dplanes, int64_t ia_begin, int64_t ia_end) {
+  const bool masked = dmask != nullptr;
+  Problem prev;
+  const double* prevVF = nullptr;
+  cudaError_t e;
+  for (int level = p->multipass - 1; level >= 0; --level) {
+    if (level > 20) return fail(ctx, MQP_ERR_INVALID, "multipass too large");
+    Problem pb;
+    int rc = resolve(ctx, p, ndims, dims, masked, 1 << level, pb);
+    if (rc != MQP_OK) return rc;
+    double* outVF = dVF;
+    double* outSN = nullptr;
+    if (level == 0) {
+      outSN = dSN;
+    } else {
+      DevBuf& b = ctx->passVF[level & 1];
+      if ((e = b.ensure((size_t)(pb.n_ia > 0 ? pb.n_ia : 1) * ndims * sizeof(double))) != cudaSuccess)
+        return cuda_fail(ctx, e, "multi-pass vector buffer");
+      outVF = (double*)b.ptr;
+    }
+    const int32_t* dpred = nullptr;
+    if (prevVF && pb.n_ia > 0) {
+      if ((e = ctx->pred.ensure((size_t)pb.n_ia * ndims * sizeof(int32_t))) != cudaSuccess)
+        return cuda_fail(ctx, e, "predictor buffer");
+      mqp::PredArgs pa;
+      memset(&pa, 0, sizeof(pa));
+      pa.ndims = ndims;
+      for (int d = 0; d < ndims; ++d) {
+        pa.vf_f[d] = (int)pb.vf[d];
+        pa.vf_c[d] = (int)prev.vf[d];
+        pa.isz_f[d] = pb.IS[d];
+        pa.st_f[d] = pb.st[d];
+        pa.isz_c[d] = prev.IS[d];
+        pa.st_c[d] = prev.st[d];
+      }
+      pa.VFc = prevVF;
+      pa.pred = (int32_t*)ctx->pred.ptr;
+      {
+        ProfileScope ps(ctx, s, 2, 0);
+        if ((e = mqp::launch_predictor(pa, s)) != cudaSuccess) return cuda_fail(ctx, e, "predictor kernel");
+      }
+      dpred = pa.pred;
+    }
+    if (pb.n_ia > 0) {
+      const int64_t b0 = level == 0 ? ia_begin : 0, b1 = level == 0 ? ia_end : pb.n_ia;
+      double* pl = level == 0 ? dplanes : nullptr;
+      rc = ndims == 3 ? run_pass_3d(ctx, pb, p, d1, d2, dmask, dskip, dtype, outVF, outSN, dpred, pl, b0, b1, s)
+                      : run_pass_2d(ctx, pb, p, d1, d2, dmask, dskip, dtype, outVF, outSN, dpred, pl, b0, b1, s);
+      if (rc != MQP_OK) return rc;
+    }
+    prev = pb;
+    prevVF = outVF;
+  }
+  return MQP_OK;
+}
+
 int piv_device_impl(mqp_ctx* ctx, const void* d1, const void* d2, const void* dmask, const void* dmask_skip,
                     int dtype, int ndims, const int64_t dims[3], const mqp_params* p, double* dVF,
                     double* dSN, cudaStream_t s, double* dplanes, int64_t ia_begin, int64_t ia_end) {
@@ -283,13 +445,17 @@ int piv_device_impl(mqp_ctx* ctx, const void* d1, const void* d2, const void* dm
   Problem pb;
   int rc = resolve(ctx, p, ndims, dims, masked, 1, pb);
   if (rc != MQP_OK) return rc;
-  if (ndims == 3) return fail(ctx, MQP_ERR_UNSUPPORTED, "3D PIV is not available in this build");
   if (pb.n_ia == 0) return MQP_OK;
   if (ia_end < 0) ia_end = pb.n_ia;
   if (ia_begin < 0 || ia_begin > ia_end || ia_end > pb.n_ia) return fail(ctx, MQP_ERR_INVALID, "IA range outside the vector field");
   if (!p->computeSN) dSN = nullptr;
+  if (p->refine && p->multipass > 1)
+    return run_multipass(ctx, p, d1, d2, dmask, dmask_skip, dtype, ndims, dims, dVF, dSN, s, dplanes, ia_begin,
+                         ia_end);
   // multipass without refinement re-runs the scale-1 geometry with identical
   // results (src/multi_quickPIV.jl:57, Q6): one pass gives the same VF/SN
+  if (ndims == 3)
+    return run_pass_3d(ctx, pb, p, d1, d2, dmask, dmask_skip, dtype, dVF, dSN, nullptr, dplanes, ia_begin, ia_end, s);
   return run_pass_2d(ctx, pb, p, d1, d2, dmask, dmask_skip, dtype, dVF, dSN, nullptr, dplanes, ia_begin, ia_end, s);
 }
 
@@ -427,6 +593,17 @@ int mqp_profile_read(mqp_ctx* ctx, mqp_profile* out) {
   ctx->spans.clear();
   *out = ctx->prof;
   return MQP_OK;
+}
+
+int mqp_set_tuning(mqp_ctx* ctx, int key, int64_t value) {
+  if (!ctx) return fail(nullptr, MQP_ERR_INVALID, "null context");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (value < 0) return fail(ctx, MQP_ERR_INVALID, "tuning values must be >= 0");
+  switch (key) {
+    case MQP_TUNE_CHUNK3D: ctx->chunk3d = value; return MQP_OK;
+    case MQP_TUNE_CHUNK3D_BUDGET: ctx->chunk3d_budget = value > 0 ? (size_t)value : ((size_t)1 << 30); return MQP_OK;
+    default: return fail(ctx, MQP_ERR_INVALID, "unknown tuning key " + std::to_string(key));
+  }
 }
 
 int mqp_correlation_planes(mqp_ctx* ctx, const void* img1, const void* img2, const void* mask,

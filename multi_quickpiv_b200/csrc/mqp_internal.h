@@ -7,6 +7,8 @@
 #include <string>
 
 #include "mqp_piv2d.cuh"
+#include "mqp_piv3d.cuh"
+#include "mqp_multipass.cuh"
 
 namespace mqp {
 
@@ -17,6 +19,12 @@ cudaError_t launch_integral2d(const void* img, int dtype, int H, int W, bool squ
                               double* out, double* scratch, cudaStream_t s);
 size_t integral2d_scratch_bytes(int H, int W);
 
+// The same for a column-major H x W x D volume: out is (H+1) x (W+1) x (D+1),
+// first plane zero; scratch holds integral3d_scratch_bytes(H, W, D) bytes.
+cudaError_t launch_integral3d(const void* img, int dtype, int H, int W, int D, bool square,
+                              double* out, double* scratch, cudaStream_t s);
+size_t integral3d_scratch_bytes(int H, int W, int D);
+
 // Smallest supported power-of-two FFT length covering the search window,
 // or 0 when the window is too large for the fused 2D kernel.
 int piv2d_fft_len(int SS1, int SS2);
@@ -26,5 +34,16 @@ int piv2d_fft_len(int SS1, int SS2);
 cudaError_t launch_piv2d(const Piv2dArgs& a, int alg, cudaStream_t s, std::string& err);
 
 int device_sm_count(int device);
+
+// 3D path: cubic FFT length for the search window (0 = unsupported), chunk
+// scratch bytes per IA, and the three-kernel launch over [a.ia_begin,
+// a.ia_end) in chunks of `chunk` IAs (the scratch pointers of `a` must hold
+// chunk IAs).
+int piv3d_fft_len(const int SS[3]);
+size_t piv3d_scratch_bytes_per_ia(const int IS[3], const int SM[3], int alg);
+cudaError_t launch_piv3d(const Piv3dArgs& a, int alg, long long chunk, cudaStream_t s, std::string& err);
+
+// Multi-pass refinement: the fine pass's predictor from the coarse vectors.
+cudaError_t launch_predictor(const PredArgs& a, cudaStream_t s);
 
 }  // namespace mqp

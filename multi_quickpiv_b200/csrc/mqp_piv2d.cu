@@ -17,11 +17,16 @@ namespace mqp {
 // pass 1: one warp per image column, prefix sum down the column (dim 1,
 // contiguous) with warp scans; writes rows 1..H of out column c+1 and the
 // zero first row.
+// blockIdx.y selects one of a batch of planes (the z slices of a volume):
+// input plane z starts at img + z*in_plane, its output at out + z*out_plane.
 template <typename T, bool SQ>
-__global__ void integral_cols_kernel(const T* __restrict__ img, int H, int W, double* __restrict__ out) {
+__global__ void integral_cols_kernel(const T* __restrict__ img, int H, int W, double* __restrict__ out,
+                                     long long in_plane, long long out_plane) {
   const int warps = blockDim.x >> 5;
   const int lane = threadIdx.x & 31;
   const long long ld = (long long)H + 1;
+  img += in_plane * blockIdx.y;
+  out += out_plane * blockIdx.y;
   for (int c = blockIdx.x * warps + (threadIdx.x >> 5); c <= W; c += gridDim.x * warps) {
     double* o = out + ld * c;
     if (c == 0) {
@@ -56,11 +61,14 @@ __global__ void integral_cols_kernel(const T* __restrict__ img, int H, int W, do
 // coalesced column segment.
 constexpr int ICHUNK = 64;
 
-__global__ void integral_rows_chunk_kernel(int H, int W, double* __restrict__ out, double* __restrict__ totals) {
+__global__ void integral_rows_chunk_kernel(int H, int W, double* __restrict__ out, double* __restrict__ totals,
+                                           long long out_plane, long long tot_plane) {
   const long long ld = (long long)H + 1;
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   const int k = blockIdx.y;
   if (r > H) return;
+  out += out_plane * blockIdx.z;
+  totals += tot_plane * blockIdx.z;
   const int c0 = 1 + k * ICHUNK;
   const int c1 = c0 + ICHUNK <= W + 1 ? c0 + ICHUNK : W + 1;
   double acc = 0.0;
@@ -84,11 +92,14 @@ __global__ void integral_rows_chunk_kernel(int H, int W, double* __restrict__ ou
 
 // pass 3: every chunk k > 0 adds the sum of the totals of chunks 0..k-1
 __global__ void integral_rows_offset_kernel(int H, int W, double* __restrict__ out,
-                                            const double* __restrict__ totals) {
+                                            const double* __restrict__ totals, long long out_plane,
+                                            long long tot_plane) {
   const long long ld = (long long)H + 1;
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   const int k = blockIdx.y + 1;
   if (r > H) return;
+  out += out_plane * blockIdx.z;
+  totals += tot_plane * blockIdx.z;
   double off = 0.0;
   for (int q = 0; q < k; ++q) off += totals[r + ld * q];
   const int c0 = 1 + k * ICHUNK;
@@ -96,29 +107,72 @@ __global__ void integral_rows_offset_kernel(int H, int W, double* __restrict__ o
   for (int c = c0; c < c1; ++c) out[r + ld * c] += off;
 }
 
-cudaError_t launch_integral2d(const void* img, int dtype, int H, int W, bool square, double* out,
-                              double* scratch, cudaStream_t s) {
+// pass 4 (volumes): running sums along dim 3, one thread per (row, column)
+// walking the planes; consecutive threads take consecutive rows.
+__global__ void integral_zscan_kernel(long long plane, int D, double* __restrict__ out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= plane) return;
+  double acc = 0.0;
+  for (int z = 1; z <= D; ++z) {
+    double* p = out + plane * z + i;
+    acc += *p;
+    *p = acc;
+  }
+}
+
+// 2D exclusive-prefix integrals of `planes` consecutive H x W planes of img,
+// plane z written to out + z*out_plane.
+static cudaError_t integral_planes(const void* img, int dtype, int H, int W, int planes, bool square, double* out,
+                                   long long out_plane, double* scratch, cudaStream_t s) {
   const int threads = 256;
   const int blocks = (W + 1 + 7) / 8 < 4096 ? (W + 1 + 7) / 8 : 4096;
+  const long long in_plane = (long long)H * W;
+  const dim3 gc(blocks, planes);
   if (dtype == 0) {
-    if (square) integral_cols_kernel<float, true><<<blocks, threads, 0, s>>>((const float*)img, H, W, out);
-    else integral_cols_kernel<float, false><<<blocks, threads, 0, s>>>((const float*)img, H, W, out);
+    if (square) integral_cols_kernel<float, true><<<gc, threads, 0, s>>>((const float*)img, H, W, out, in_plane, out_plane);
+    else integral_cols_kernel<float, false><<<gc, threads, 0, s>>>((const float*)img, H, W, out, in_plane, out_plane);
   } else {
-    if (square) integral_cols_kernel<double, true><<<blocks, threads, 0, s>>>((const double*)img, H, W, out);
-    else integral_cols_kernel<double, false><<<blocks, threads, 0, s>>>((const double*)img, H, W, out);
+    if (square) integral_cols_kernel<double, true><<<gc, threads, 0, s>>>((const double*)img, H, W, out, in_plane, out_plane);
+    else integral_cols_kernel<double, false><<<gc, threads, 0, s>>>((const double*)img, H, W, out, in_plane, out_plane);
   }
   const int chunks = (W + ICHUNK - 1) / ICHUNK;
-  const dim3 g1((H + 1 + 127) / 128, chunks);
-  integral_rows_chunk_kernel<<<g1, 128, 0, s>>>(H, W, out, scratch);
+  const long long tot_plane = (long long)(H + 1) * (chunks + 1);
+  const dim3 g1((H + 1 + 127) / 128, chunks, planes);
+  integral_rows_chunk_kernel<<<g1, 128, 0, s>>>(H, W, out, scratch, out_plane, tot_plane);
   if (chunks > 1) {
-    const dim3 g2((H + 1 + 127) / 128, chunks - 1);
-    integral_rows_offset_kernel<<<g2, 128, 0, s>>>(H, W, out, scratch);
+    const dim3 g2((H + 1 + 127) / 128, chunks - 1, planes);
+    integral_rows_offset_kernel<<<g2, 128, 0, s>>>(H, W, out, scratch, out_plane, tot_plane);
   }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_integral2d(const void* img, int dtype, int H, int W, bool square, double* out,
+                              double* scratch, cudaStream_t s) {
+  return integral_planes(img, dtype, H, W, 1, square, out, 0, scratch, s);
+}
+
+cudaError_t launch_integral3d(const void* img, int dtype, int H, int W, int D, bool square, double* out,
+                              double* scratch, cudaStream_t s) {
+  const long long plane = (long long)(H + 1) * (W + 1);
+  cudaError_t e = cudaMemsetAsync(out, 0, (size_t)plane * sizeof(double), s);
+  if (e != cudaSuccess) return e;
+  // planes are independent in the 2D passes; the grid's y/z extent bounds a batch
+  for (int z0 = 0; z0 < D; z0 += 65535) {
+    const int nz = D - z0 < 65535 ? D - z0 : 65535;
+    const char* src = (const char*)img + (size_t)z0 * H * W * (dtype == 0 ? 4 : 8);
+    e = integral_planes(src, dtype, H, W, nz, square, out + plane * (1 + z0), plane, scratch, s);
+    if (e != cudaSuccess) return e;
+  }
+  integral_zscan_kernel<<<(unsigned)((plane + 255) / 256), 256, 0, s>>>(plane, D, out);
   return cudaGetLastError();
 }
 
 size_t integral2d_scratch_bytes(int H, int W) {
   return (size_t)(H + 1) * (size_t)((W + ICHUNK - 1) / ICHUNK + 1) * sizeof(double);
+}
+
+size_t integral3d_scratch_bytes(int H, int W, int D) {
+  return integral2d_scratch_bytes(H, W) * (size_t)(D < 65535 ? D : 65535);
 }
 
 // ---------------------------------------------------------------------------

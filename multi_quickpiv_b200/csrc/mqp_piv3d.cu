@@ -1,0 +1,247 @@
+// sm_100a kernels of the 3D path (see mqp_piv3d.cuh): K3a (r2c along dim 3),
+// K3b (complex 2D correlation per k3 slab), K3c (inverse along k3, similarity,
+// peak, Gaussian fit, SN), launched chunk by chunk over the vector field.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "mqp_internal.h"
+
+namespace mqp {
+
+namespace {
+
+constexpr int K3A_THREADS = 256;
+constexpr int K3C_THREADS = 256;
+
+__device__ __forceinline__ double warp_sum3(double v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  return v;
+}
+__device__ __forceinline__ double warp_max3(double v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, off));
+  return v;
+}
+__device__ __forceinline__ double warp_nmax3(double v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v = nmax(v, __shfl_xor_sync(0xffffffffu, v, off));
+  return v;
+}
+
+// One block per IA of the chunk; threads walk the IA's lines.
+template <int N, bool FPRUNE, int ALG, typename T>
+__global__ void __launch_bounds__(K3A_THREADS) k3a_kernel(Piv3dArgs a, int pass) {
+  const long long ci = blockIdx.x;
+  const IAGeom3 g = ia_geom3(a, a.ia_begin + ci);
+  IA3State s;
+  if (pass == 0) {
+    ia3_means<ALG>(a, g, s.meanF, s.meanG);
+    s.sumF2 = 0.0;
+    s.skip = 0;
+  } else {
+    s = a.state[ci];
+  }
+  double vmax = -INFINITY, mmax = -INFINITY, sumsq = 0.0;
+  const int nl = k3a_lines(a, g);
+  for (int line = threadIdx.x; line < nl; line += K3A_THREADS)
+    k3a_line<N, FPRUNE, T, ALG>(a, g, s, pass, ci, line, vmax, mmax, sumsq);
+  if (pass != 0) return;
+  __shared__ double red[3][K3A_THREADS / 32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  vmax = warp_max3(vmax);
+  mmax = warp_max3(mmax);
+  sumsq = warp_sum3(sumsq);
+  if (lane == 0) {
+    red[0][warp] = vmax;
+    red[1][warp] = mmax;
+    red[2][warp] = sumsq;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < K3A_THREADS / 32; ++w) {
+      vmax = fmax(vmax, red[0][w]);
+      mmax = fmax(mmax, red[1][w]);
+      sumsq += red[2][w];
+    }
+    s.sumF2 = sumsq;
+    s.skip = skip_test3(a, ALG, vmax, mmax) ? 1 : 0;
+    a.state[ci] = s;
+  }
+}
+
+// One block of N threads per (k3, IA) slab.
+template <int N, bool FPRUNE>
+__global__ void __launch_bounds__(N) k3b_kernel(Piv3dArgs a, float2* C) {
+  using L = Lay3<N, FPRUNE>;
+  extern __shared__ float2 sm[];
+  const int k3 = blockIdx.x;
+  const long long ci = blockIdx.y;
+  if (a.state[ci].skip) return;
+  const IAGeom3 g = ia_geom3(a, a.ia_begin + ci);
+  const int P1 = 2 * a.SM[0] + 1, P2 = 2 * a.SM[1] + 1;
+  float2* S = sm;
+  float2* SF = sm + N * L::SSTR;
+  const int t = threadIdx.x;
+  k3b_rows<N, FPRUNE>(a, g, ci, k3, t, S, SF);
+  __syncthreads();
+  float2 p[N];
+  k3b_cols<N, FPRUNE>(t, S, SF, p);
+  __syncthreads();
+  k3b_store_cols<N, FPRUNE>(t, P1, p, S);
+  __syncthreads();
+  k3b_rows2<N, FPRUNE>(ci, k3, t, P1, P2, S, C);
+}
+
+// One block per IA of the chunk.
+template <int N, int ALG>
+__global__ void __launch_bounds__(K3C_THREADS) k3c_kernel(Piv3dArgs a) {
+  const long long ci = blockIdx.x;
+  const int P1 = 2 * a.SM[0] + 1, P2 = 2 * a.SM[1] + 1, P3 = 2 * a.SM[2] + 1;
+  const IA3State s = a.state[ci];
+  if (s.skip) {
+    if (threadIdx.x == 0) k3c_skipped(a, ci);
+    if (a.planes) {
+      const long long vol = (long long)P1 * P2 * P3;
+      double* dst = a.planes + (a.ia_begin + ci - a.planes_begin) * vol;
+      for (long long i = threadIdx.x; i < vol; i += K3C_THREADS) dst[i] = 0.0;
+    }
+    return;
+  }
+  const IAGeom3 g = ia_geom3(a, a.ia_begin + ci);
+  const LagRanges3 R = lag_ranges3(a, g);
+  PeakAcc acc;
+  acc.best = 0.0;
+  acc.bidx = -1;
+  acc.smax = -INFINITY;
+  acc.ssum = 0.0;
+  for (int q = threadIdx.x; q < P1 * P2; q += K3C_THREADS) k3c_pair<N, ALG>(a, g, s, ci, q, P1, P2, P3, R, acc);
+  // block merge: (largest value, lowest column-major index), NaN-propagating max, sum
+  __shared__ double rb[K3C_THREADS / 32], rs[K3C_THREADS / 32], rm[K3C_THREADS / 32];
+  __shared__ int ri[K3C_THREADS / 32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double best = acc.best;
+  int bidx = acc.bidx;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    const double ob = __shfl_xor_sync(0xffffffffu, best, off);
+    const int oi = __shfl_xor_sync(0xffffffffu, bidx, off);
+    peak_merge(best, bidx, ob, oi);
+  }
+  const double smax = warp_nmax3(acc.smax);
+  const double ssum = warp_sum3(acc.ssum);
+  if (lane == 0) {
+    rb[warp] = best;
+    ri[warp] = bidx;
+    rm[warp] = smax;
+    rs[warp] = ssum;
+  }
+  __syncthreads();  // also publishes the similarity volume to thread 0
+  if (threadIdx.x == 0) {
+    double b = rb[0], mx = rm[0], sum = rs[0];
+    int bi = ri[0];
+    for (int w = 1; w < K3C_THREADS / 32; ++w) {
+      peak_merge(b, bi, rb[w], ri[w]);
+      mx = nmax(mx, rm[w]);
+      sum += rs[w];
+    }
+    k3c_final(a, g, ci, R, b, bi, mx, sum);
+  }
+}
+
+template <int N, bool FPRUNE, int ALG, typename T>
+cudaError_t run_chunks(Piv3dArgs a, long long chunk, cudaStream_t s, std::string& err) {
+  using L = Lay3<N, FPRUNE>;
+  const size_t smem = (size_t)L::SMEM_F2 * sizeof(float2);
+  cudaError_t e = cudaFuncSetAttribute(k3b_kernel<N, FPRUNE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) {
+    err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e);
+    return e;
+  }
+  const long long begin = a.ia_begin, end = a.ia_end;
+  constexpr int NPASS = ALG == ALG_MASK_NSQECC ? 2 : 1;
+  for (long long c0 = begin; c0 < end; c0 += chunk) {
+    const long long n = end - c0 < chunk ? end - c0 : chunk;
+    a.ia_begin = c0;
+    a.ia_end = c0 + n;
+    for (int pass = 0; pass < NPASS; ++pass) {
+      k3a_kernel<N, FPRUNE, ALG, T><<<(unsigned)n, K3A_THREADS, 0, s>>>(a, pass);
+      k3b_kernel<N, FPRUNE><<<dim3(L::K3, (unsigned)n), N, smem, s>>>(a, pass == 0 ? a.C : a.C2);
+    }
+    k3c_kernel<N, ALG><<<(unsigned)n, K3C_THREADS, 0, s>>>(a);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      err = std::string("piv3d launch: ") + cudaGetErrorString(e);
+      return e;
+    }
+  }
+  return cudaSuccess;
+}
+
+template <int N, bool FPRUNE, typename T>
+cudaError_t run_alg(const Piv3dArgs& a, int alg, long long chunk, cudaStream_t s, std::string& err) {
+  switch (alg) {
+    case ALG_FFTCC: return run_chunks<N, FPRUNE, ALG_FFTCC, T>(a, chunk, s, err);
+    case ALG_ZNCC: return run_chunks<N, FPRUNE, ALG_ZNCC, T>(a, chunk, s, err);
+    case ALG_NSQECC: return run_chunks<N, FPRUNE, ALG_NSQECC, T>(a, chunk, s, err);
+    case ALG_MASK_NSQECC: return run_chunks<N, FPRUNE, ALG_MASK_NSQECC, T>(a, chunk, s, err);
+    default: err = "unknown correlation algorithm"; return cudaErrorInvalidValue;
+  }
+}
+
+template <int N, bool FPRUNE>
+cudaError_t run_dt(const Piv3dArgs& a, int alg, long long chunk, cudaStream_t s, std::string& err) {
+  return a.dtype == 0 ? run_alg<N, FPRUNE, float>(a, alg, chunk, s, err)
+                      : run_alg<N, FPRUNE, double>(a, alg, chunk, s, err);
+}
+
+}  // namespace
+
+int piv3d_fft_len(const int SS[3]) {
+  int m = SS[0];
+  if (SS[1] > m) m = SS[1];
+  if (SS[2] > m) m = SS[2];
+  if (m <= 32) return 32;
+  if (m <= 64) return 64;
+  return 0;
+}
+
+static bool piv3d_prune(const int IS[3], int N) { return IS[0] <= N / 2 && IS[1] <= N / 2 && IS[2] <= N / 2; }
+
+size_t piv3d_scratch_bytes_per_ia(const int IS[3], const int SM[3], int alg) {
+  const int SS[3] = {IS[0] + 2 * SM[0], IS[1] + 2 * SM[1], IS[2] + 2 * SM[2]};
+  const int N = piv3d_fft_len(SS);
+  if (N == 0) return 0;
+  const size_t K3 = N / 2 + 1;
+  const size_t NF = piv3d_prune(IS, N) ? N / 2 : N;
+  const size_t P12 = (size_t)(2 * SM[0] + 1) * (2 * SM[1] + 1);
+  const size_t P3 = 2 * SM[2] + 1;
+  const size_t ncorr = alg == ALG_MASK_NSQECC ? 2 : 1;
+  size_t b = 0;
+  b += K3 * N * N * sizeof(float2);        // Gz
+  b += K3 * NF * NF * sizeof(float2);      // Fz
+  b += ncorr * K3 * P12 * sizeof(float2);  // C (and C2)
+  b += P12 * P3 * sizeof(float);           // V
+  b += sizeof(IA3State);
+  return b + 6 * 256;                      // alignment of the six arrays
+}
+
+cudaError_t launch_piv3d(const Piv3dArgs& a, int alg, long long chunk, cudaStream_t s, std::string& err) {
+  const int SS[3] = {a.IS[0] + 2 * a.SM[0], a.IS[1] + 2 * a.SM[1], a.IS[2] + 2 * a.SM[2]};
+  const int N = piv3d_fft_len(SS);
+  if (chunk < 1 || chunk > 65535) {
+    err = "3D chunk must be in [1, 65535]";
+    return cudaErrorInvalidValue;
+  }
+  if (a.ia_end <= a.ia_begin) return cudaSuccess;
+  const bool prune = piv3d_prune(a.IS, N);
+  if (N == 64) return prune ? run_dt<64, true>(a, alg, chunk, s, err) : run_dt<64, false>(a, alg, chunk, s, err);
+  if (N == 32) return prune ? run_dt<32, true>(a, alg, chunk, s, err) : run_dt<32, false>(a, alg, chunk, s, err);
+  err = "3D search window (interSize + 2 searchMargin) above 64 along some axis is not supported";
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace mqp

@@ -623,6 +623,8 @@ def predictor_from_coarse(VFc, scale_c, size, p, scale_f):
     isz_f, st_f = _isize(p, scale_f), _step(p, scale_f)
     vf_f = get_vectorfield_size(size, isz_f, st_f)
     vf_c = VFc.shape[1:]
+    if any(v == 0 for v in vf_c):  # the coarse pass had no IA: no shift
+        return np.zeros((N,) + vf_f, dtype=np.int64)
     idx = []
     for d in range(N):
         jf = np.arange(vf_f[d])

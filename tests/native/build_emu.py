@@ -1,5 +1,5 @@
 """Builds tests/_native/libmqp_emu.so, the host emulation of the 2D kernel
-used by the CPU tests (see mqp_emu.cu)."""
+and of the 3D kernels used by the CPU tests (see mqp_emu.cu, mqp_emu3d.cu)."""
 import os
 import subprocess
 import sys
@@ -11,13 +11,13 @@ OUT = os.path.join(os.path.dirname(HERE), "_native", "libmqp_emu.so")
 
 
 def build(force=False):
-    src = os.path.join(HERE, "mqp_emu.cu")
-    deps = [src] + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".inc"))]
+    srcs = [os.path.join(HERE, f) for f in ("mqp_emu.cu", "mqp_emu3d.cu")]
+    deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".inc"))]
     if not force and os.path.exists(OUT) and all(os.path.getmtime(d) <= os.path.getmtime(OUT) for d in deps):
         return OUT
     os.makedirs(os.path.dirname(OUT), exist_ok=True)
     cmd = ["nvcc", "-std=c++17", "-O2", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-fvisibility=hidden",
-           "-shared", "-I", CSRC, src, "-o", OUT]
+           "-shared", "-I", CSRC] + srcs + ["-o", OUT]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(r.stdout + r.stderr)

@@ -1,0 +1,52 @@
+"""GPU multi-pass refinement (mqp_params.refine) against the oracle's
+refined multipass, 2D and 3D, through the C ABI."""
+import numpy as np
+import pytest
+
+import oracle.piv_oracle as O
+from multi_quickpiv_b200 import PIV, setPIVParameters, synth
+from tests.helpers import VF_ATOL, sn_ok
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(i1, i2, alg, IS, SM, st, passes, mask=None):
+    po = O.set_piv_parameters(corr_alg=alg, interSize=IS, searchMargin=SM, step=st, multipass=passes,
+                              computeSN=True)
+    VFo, SNo = O.PIV(i1, i2, po, mask=mask, refine=True)
+    pp = setPIVParameters(corr_alg=alg, interSize=IS, searchMargin=SM, step=st, multipass=passes, computeSN=True,
+                          refine=True)
+    VF, SN = PIV(i1, i2, *([mask] if mask is not None else []), pp)
+    assert VF.shape == VFo.shape
+    bad = (np.abs(VF - VFo) > VF_ATOL).any(axis=0)
+    # a coarse-pass near-tie can move one fine predictor; none occur on these inputs
+    assert bad.sum() == 0, (np.argwhere(bad)[:5], np.abs(VF - VFo).max())
+    assert sn_ok(SN, SNo).all()
+    return VF
+
+
+@pytest.mark.parametrize("alg", ["fft", "zncc", "nsqecc"])
+def test_two_pass_2d_large_shift(alg, gpu):
+    i1, i2, _ = synth.pair_2d_shift(shape=(160, 176), shift=(9.4, -6.2), seed_stream=40, dtype=np.float32)
+    VF = _run(i1, i2, alg, (16, 16), (4, 4), (16, 16), 2)
+    inner = VF[:, 1:-1, 1:-1]
+    assert abs(np.median(inner[0]) - 9.4) < 0.1 and abs(np.median(inner[1]) + 6.2) < 0.1
+
+
+def test_three_pass_2d(gpu):
+    i1, i2, _ = synth.pair_2d_vortex(shape=(192, 160), core=40.0, peak=7.0)
+    _run(i1, i2, "nsqecc", (8, 8), (4, 4), (8, 8), 3)
+
+
+def test_two_pass_2d_masked(gpu):
+    i1, i2, _ = synth.pair_2d_shift(shape=(128, 128), shift=(6.3, 5.1), seed_stream=41)
+    mask = synth.ellipse_mask(np.random.default_rng(8), i1.shape, cover=0.8)
+    _run(i1, i2, "nsqecc", (16, 16), (4, 4), (16, 16), 2, mask=mask)
+
+
+@pytest.mark.parametrize("alg", ["fft", "nsqecc"])
+def test_two_pass_3d(alg, gpu):
+    i1, i2, _ = synth.pair_3d_shear(shape=(96, 80, 80), seed_stream=42, shift=(5.6, -4.3, 2.2), shear=0.0)
+    VF = _run(i1, i2, alg, (16, 16, 16), (8, 8, 8), (16, 16, 16), 2)
+    inner = VF[:, 1:-1, 1:-1, 1:-1]
+    assert abs(np.median(inner[0]) - 5.6) < 0.1

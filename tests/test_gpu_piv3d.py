@@ -1,0 +1,151 @@
+"""GPU parity of the 3D kernels against the Float64 oracle and the committed
+3D golden fixtures, through the C ABI (multi_quickpiv_b200.PIV -> mqp_piv),
+and the 512x512x256 FFTCC workload against the C++ restatement on sampled
+interrogation areas."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import oracle.cpu_ref as CR
+import oracle.piv_oracle as O
+from multi_quickpiv_b200 import PIV, correlation_planes, setPIVParameters, synth
+from tests.helpers import MASK_PLANE_RTOL, PLANE_RTOL, VF_ATOL, compare_planes, mask_coverage, sn_ok
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN3D = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*3d*.npz")))
+
+
+def _params(alg, IS, SM, st, thr=-1.0):
+    return setPIVParameters(corr_alg=alg, interSize=IS, searchMargin=SM, step=st, computeSN=True, threshold=thr)
+
+
+def _check(VF, SN, planes, VFo, SNo, corr, shape, IS, SM, st, rtol=PLANE_RTOL, skip=None):
+    assert VF.shape == VFo.shape
+    worst, near_tie = compare_planes(planes, corr, shape, IS, SM, st, skip=skip)
+    assert worst <= rtol, worst
+    bad = (np.abs(VF - VFo) > VF_ATOL).any(axis=0) & ~near_tie
+    assert not bad.any(), (np.argwhere(bad)[:5], np.abs(VF - VFo).max())
+    if SN is not None:
+        assert (sn_ok(SN, SNo) | near_tie).all()
+
+
+@pytest.mark.parametrize("path", GOLDEN3D, ids=lambda p: os.path.basename(p)[:-4])
+def test_piv3d_reproduces_golden(path, gpu):
+    z = np.load(path)
+    IS, SM, st = (tuple(int(v) for v in z[k]) for k in ("interSize", "searchMargin", "step"))
+    pp = _params(str(z["alg"]), IS, SM, st, float(z["threshold"]))
+    VF, SN = PIV(z["img1"], z["img2"], pp)
+    planes = correlation_planes(z["img1"], z["img2"], pp)
+    vf = VF.shape[1:]
+    corr = {k: z["planes"][..., int(np.ravel_multi_index(k, vf, order="F"))] for k in np.ndindex(*vf)}
+    _check(VF, SN, planes, z["VF"], z["SN"], corr, z["img1"].shape, IS, SM, st)
+
+
+CASES = [
+    ((40, 36, 40), (16, 16, 16), (8, 8, 8), (12, 10, 12)),
+    ((72, 64, 64), (32, 32, 32), (16, 16, 16), (16, 16, 16)),
+    ((36, 36, 30), (24, 20, 18), (4, 6, 4), (6, 8, 6)),
+    ((48, 40, 44), (16, 12, 20), (8, 10, 6), (16, 14, 12)),
+]
+
+
+@pytest.mark.parametrize("alg", ["fft", "zncc", "nsqecc"])
+@pytest.mark.parametrize("cfg", CASES, ids=["n32", "n64", "n32full", "aniso"])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_piv3d_matches_oracle(alg, cfg, dtype, gpu):
+    shape, IS, SM, st = cfg
+    i1, i2, _ = synth.pair_3d_shear(shape=shape, seed_stream=31, dtype=dtype)
+    po = O.set_piv_parameters(corr_alg=alg, interSize=IS, searchMargin=SM, step=st, computeSN=True)
+    po.ndims = 3
+    VFo, SNo, Co = O.piv_single_pass(i1, i2, po, keep_corr=True)
+    pp = _params(alg, IS, SM, st)
+    VF, SN = PIV(i1, i2, pp)
+    planes = correlation_planes(i1, i2, pp)
+    _check(VF, SN, planes, VFo, SNo, Co, shape, IS, SM, st)
+
+
+def test_piv3d_masked(gpu):
+    shape, IS, SM, st = (48, 44, 40), (16, 16, 16), (8, 8, 8), (8, 8, 8)
+    i1, i2, _ = synth.pair_3d_shear(shape=shape, seed_stream=32, dtype=np.float64)
+    mask = synth.ellipse_mask(np.random.default_rng(5), shape, cover=0.7)
+    po = O.set_piv_parameters(interSize=IS, searchMargin=SM, step=st, computeSN=True)
+    po.ndims = 3
+    VFo, SNo, Co = O.piv_single_pass(i1, i2, po, mask=mask, keep_corr=True)
+    pp = _params("nsqecc", IS, SM, st)
+    VF, SN = PIV(i1, i2, mask, pp)
+    planes = correlation_planes(i1, i2, pp, mask=mask)
+    sparse = mask_coverage(mask, shape, IS, st) < 0.25
+    worst, near_tie = compare_planes(planes, Co, shape, IS, SM, st, skip=sparse)
+    assert worst <= MASK_PLANE_RTOL, worst
+    bad = (np.abs(VF - VFo) > VF_ATOL).any(axis=0) & ~near_tie
+    assert not bad.any(), np.abs(VF - VFo).max()
+
+
+def test_piv3d_threshold_skip(gpu):
+    shape, IS, SM, st = (40, 40, 40), (16, 16, 16), (8, 8, 8), (12, 12, 12)
+    i1, i2, _ = synth.pair_3d_shear(shape=shape, seed_stream=33, dtype=np.float64)
+    i1 = i1.copy()
+    i1[:16, :16, :16] = -50.0
+    VF, SN = PIV(i1, i2, _params("fft", IS, SM, st, thr=0.0))
+    assert np.all(VF[:, 0, 0, 0] == 0) and SN[0, 0, 0] == 0
+    po = O.set_piv_parameters(corr_alg="fft", interSize=IS, searchMargin=SM, step=st, computeSN=True, threshold=0.0)
+    po.ndims = 3
+    VFo, _ = O.piv_single_pass(i1, i2, po)
+    assert np.max(np.abs(VF - VFo)) < VF_ATOL
+
+
+def test_piv3d_chunking_is_invisible(gpu):
+    """Chunk boundaries of the 3D launch do not change any vector."""
+    import multi_quickpiv_b200._lib as L
+    shape, IS, SM, st = (72, 64, 64), (32, 32, 32), (16, 16, 16), (16, 16, 16)
+    i1, i2, _ = synth.pair_3d_shear(shape=shape, seed_stream=34)
+    pp = _params("nsqecc", IS, SM, st)
+    ref, sref = PIV(i1, i2, pp)
+    ctx = L.Context(0)
+    try:
+        ctx.set_chunk3d(5)
+        VF, SN = PIV(i1, i2, pp, context=ctx)
+    finally:
+        ctx.close()
+    assert np.array_equal(VF, ref) and np.array_equal(SN, sref)
+
+
+def test_piv3d_torch_device_path(gpu):
+    import torch
+    shape, IS, SM, st = (40, 36, 40), (16, 16, 16), (8, 8, 8), (12, 10, 12)
+    i1, i2, _ = synth.pair_3d_shear(shape=shape, seed_stream=35)
+    pp = _params("zncc", IS, SM, st)
+    VF, SN = PIV(i1, i2, pp)
+    VFd, SNd = PIV(torch.from_numpy(i1).cuda(), torch.from_numpy(i2).cuda(), pp)
+    assert np.array_equal(VFd.cpu().numpy(), VF) and np.array_equal(SNd.cpu().numpy(), SN)
+
+
+def test_shear_workload_512x512x256_fftcc(gpu):
+    """The 512x512x256 Float32 FFTCC workload (IS 32, SM 16, step 16; 14,415
+    IAs): every vector of two sampled IA ranges (the first z layer's border
+    and a block in the middle) equals the C++ Float64 restatement's, and the
+    interior recovers the imposed shift plus shear."""
+    CR.build()
+    i1, i2, (shift, shear) = synth.pair_3d_shear()
+    IS, SM, st = (32, 32, 32), (16, 16, 16), (16, 16, 16)
+    pp = _params("fft", IS, SM, st)
+    VF, SN = PIV(i1, i2, pp)
+    assert VF.shape == (3, 31, 31, 15)
+    vf = VF.shape[1:]
+    cp = pp.to_c()
+    for a, b in ((0, 200), (7000, 7200)):
+        VFc, SNc = CR.piv(i1, i2, cp, ia_begin=a, ia_end=b)
+        for ia in range(a, b):
+            k = np.unravel_index(ia, vf, order="F")
+            assert np.all(np.abs(VF[(slice(None),) + k] - VFc[(slice(None),) + k]) <= VF_ATOL), (ia, k)
+            assert abs(SN[k] - SNc[k]) <= 1e-4 * abs(SNc[k]) + SNc[k] ** 2 * 1e-6
+    # interior: u1 = 1.5 + 0.01 z at the IA centre, u2 = -0.8, u3 = 0.6
+    inner = VF[:, 2:-2, 2:-2, 2:-2]
+    zc = (np.arange(vf[2]) * 16 + 15.5)[2:-2]
+    assert np.abs(np.median(inner[1]) - shift[1]) < 0.05
+    assert np.abs(np.median(inner[2]) - shift[2]) < 0.05
+    u1 = np.median(inner[0], axis=(0, 1))
+    assert np.max(np.abs(u1 - (shift[0] + shear * zc))) < 0.1
