@@ -1,11 +1,13 @@
 """Benchmark of the PIV hot path: interrogation-area (IA) correlations/s.
 
-Workload (default): the 2048x2048 Float32 Lamb-Oseen vortex pair with ramp and
-gain, interSize 32, searchMargin 16, step 8 (64,009 IAs per pair), NSQECC
-(the reference's default algorithm; --alg zncc for ZNCC).  One step = one PIV
-of one image pair.
+Workload (default, --workload vortex2048): the 2048x2048 Float32 Lamb-Oseen
+vortex pair with ramp and gain, interSize 32, searchMargin 16, step 8 (64,009
+IAs per pair), NSQECC (the reference's default algorithm; --alg zncc for
+ZNCC).  --workload shear3d: the 512x512x256 Float32 volume pair (uniform shift
+plus du/dz shear), FFTCC, interSize 32^3, searchMargin 16^3, step 16^3 (14,415
+IAs).  One step = one PIV of one image pair.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload W]
 
 Under torchrun every rank runs an independent replica (the path shards by
 image pair with no exchange); the step time is the max over ranks and
@@ -33,14 +35,14 @@ METRIC = "IA correlations/s"
 UNIT = "IA/s"
 
 
-def flops_per_ia(cs=64, P=33, IS=32, norm=True):
-    """Reference-equivalent FLOPs of one 2D IA correlation (unpruned r2c/c2r of
-    size cs^2, conj-multiply, peak scan; +normalisation for ZNCC/NSQECC)."""
-    Nc = cs * cs
-    B = (cs // 2 + 1) * cs
-    f = 3 * 2.5 * Nc * math.log2(Nc) + 6 * B + P * P
+def flops_per_ia(cs=64, P=33, IS=32, norm=True, nd=2):
+    """Reference-equivalent FLOPs of one IA correlation (unpruned r2c/c2r of
+    size cs^nd, conj-multiply, peak scan; +normalisation for ZNCC/NSQECC)."""
+    Nc = cs ** nd
+    B = (cs // 2 + 1) * cs ** (nd - 1)
+    f = 3 * 2.5 * Nc * math.log2(Nc) + 6 * B + P ** nd
     if norm:
-        f += 12 * P * P + 2 * IS * IS
+        f += 12 * P ** nd + 2 * IS ** nd
     return f
 
 
@@ -111,42 +113,55 @@ def dist_env():
             int(os.environ.get("WORLD_SIZE", 1)))
 
 
-def make_workload(args):
-    from multi_quickpiv_b200 import synth
-    i1, i2, _ = synth.pair_2d_vortex(shape=(args.size, args.size))
-    return i1, i2
+class Workload:
+    """One bench workload: the image pair, its parameters and its counts."""
 
-
-def params_for(args):
-    from multi_quickpiv_b200 import setPIVParameters
-    return setPIVParameters(corr_alg=args.alg, interSize=(32, 32), searchMargin=(16, 16), step=(8, 8),
-                            computeSN=False)
+    def __init__(self, args):
+        from multi_quickpiv_b200 import setPIVParameters, synth
+        self.name = args.workload
+        if args.workload == "shear3d":
+            # 512x512x256 Float32 volumes, uniform shift + du/dz shear, FFTCC, IS 32 SM 16 step 16
+            self.i1, self.i2, _ = synth.pair_3d_shear()
+            self.alg = "fft"
+            self.IS, self.SM, self.step = 32, 16, 16
+            self.desc = "shear pair 512x512x256 float32, fft, IS 32 SM 16 step 16"
+        else:
+            self.i1, self.i2, _ = synth.pair_2d_vortex(shape=(args.size, args.size))
+            self.alg = args.alg
+            self.IS, self.SM, self.step = 32, 16, 8
+            self.desc = f"vortex pair {args.size}x{args.size} float32, {args.alg}, IS 32 SM 16 step 8"
+        self.nd = self.i1.ndim
+        self.params = setPIVParameters(corr_alg=self.alg, interSize=(self.IS,) * self.nd,
+                                       searchMargin=(self.SM,) * self.nd, step=(self.step,) * self.nd,
+                                       computeSN=False)
+        self.params.ndims = self.nd
+        self.vf = tuple((n - self.IS) // self.step + 1 for n in self.i1.shape)
+        self.n_ia = int(np.prod(self.vf))
+        norm = self.alg != "fft"
+        self.flop_per_ia = flops_per_ia(cs=64, P=2 * self.SM + 1, IS=self.IS, norm=norm, nd=self.nd)
+        npx = int(np.prod(self.i1.shape))
+        ii = int(np.prod([n + 1 for n in self.i1.shape])) * 8
+        # algorithmic bytes of one pass: both images once, the FP64 integral
+        # image of img2^2 once (ZNCC: three), the vectors out
+        self.alg_bytes = 2 * npx * 4 + (ii * (3 if self.alg == "zncc" else 1) if norm else 0) + self.n_ia * 8 * self.nd
+        self.image_bytes = npx * 4
 
 
 # ---------------------------------------------------------------------------
-def cpu_baseline_sample(i1, i2, args, budget_s=12.0):
+def cpu_baseline_sample(wl, budget_s=12.0):
     """The oracle restatement timed on this host on a bounded sample of the
     workload's IAs; returns IA/s, threads used and the sample description."""
     import oracle.cpu_ref as cref
-    if cref.available():
-        return cref.time_sample(i1, i2, args.alg, budget_s=budget_s)
-    import oracle.piv_oracle as O
-    p = O.set_piv_parameters(corr_alg=args.alg, interSize=(32, 32), searchMargin=(16, 16), step=(8, 8))
-    p.ndims = 2
-    sub1, sub2 = i1[:288, :288].astype(np.float64), i2[:288, :288].astype(np.float64)
-    t0 = time.perf_counter()
-    VF, _ = O.piv_single_pass(sub1, sub2, p)
-    dt = time.perf_counter() - t0
-    n = VF.shape[1] * VF.shape[2]
-    return {"value": n / dt, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"NumPy Float64 oracle, {n} IAs of a 288x288 crop, {dt:.1f} s"}
+    if not cref.available():
+        cref.build()
+    return cref.time_sample(wl.i1, wl.i2, wl.alg, budget_s=budget_s, IS=wl.IS, SM=wl.SM, step=wl.step)
 
 
 def run_reference(args):
     rank, local, world = dist_env()
     if rank != 0:
         return 0
-    i1, i2 = make_workload(args)
+    wl = Workload(args)
     import oracle.cpu_ref as cref
     if not cref.available():
         cref.build()
@@ -154,17 +169,16 @@ def run_reference(args):
     res = None
     times = []
     for it in range(W + K):
-        r = cref.time_sample(i1, i2, args.alg, budget_s=args.ref_budget)
+        r = cref.time_sample(wl.i1, wl.i2, wl.alg, budget_s=args.ref_budget, IS=wl.IS, SM=wl.SM, step=wl.step)
         if it >= W:
             times.append(r)
         res = r
     vals = [r["value"] for r in times]
     value = statistics.mean(vals)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
-            "ms_per_step": 1e3 * args.n_ia_full / value, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": 1e3 * wl.n_ia / value, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"vortex pair {args.size}x{args.size} float32, {args.alg}, IS 32 SM 16 step 8",
-                       "n_ia_per_pair": args.n_ia_full},
+            "config": {"workload": wl.desc, "n_ia_per_pair": wl.n_ia},
             "impl": "reference",
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": res["cores"], "kind": res["kind"],
                              "sample": res["sample"]},
@@ -174,7 +188,23 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------
+def kernel_launches(wl, chunk3d):
+    """Kernels of this library one PIV call launches (counted from the code
+    path: integral scans, the fused 2D kernel or the three 3D kernels per
+    chunk)."""
+    scans = 0
+    if wl.alg != "fft":
+        per_image = 3 if wl.nd == 2 else 4  # cols, row chunks, row offsets (+ z scan)
+        scans = per_image * (3 if wl.alg == "zncc" else 1)
+    if wl.nd == 2:
+        return scans + 1
+    chunks = -(-wl.n_ia // chunk3d)
+    return scans + 3 * chunks
+
+
 def run_ours(args):
+    import ctypes as C
+
     import torch
     import torch.distributed as dist
     rank, local, world = dist_env()
@@ -183,31 +213,33 @@ def run_ours(args):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     import multi_quickpiv_b200 as mq
-    from multi_quickpiv_b200 import _lib
+    from multi_quickpiv_b200 import _lib, tune
     ctx = _lib.Context(local)
-    i1, i2 = make_workload(args)
-    params = params_for(args)
-    params.ndims = 2
-    H, Wd = i1.shape
-    vf = mq.get_vectorfield_size(i1.shape, params)
-    n_ia = vf[0] * vf[1]
+    wl = Workload(args)
+    shape, nd, n_ia = wl.i1.shape, wl.nd, wl.n_ia
 
     # device-resident inputs (column-major, Julia order)
-    d1 = mq.piv._colmajor_torch(torch.from_numpy(i1).to(dev))
-    d2 = mq.piv._colmajor_torch(torch.from_numpy(i2).to(dev))
-    VF = torch.zeros((vf[1], vf[0], 2), dtype=torch.float64, device=dev)
-    cp = params.to_c()
-    import ctypes as C
-    dims = (C.c_int64 * 3)(H, Wd, 1)
+    d1 = mq.piv._colmajor_torch(torch.from_numpy(wl.i1).to(dev))
+    d2 = mq.piv._colmajor_torch(torch.from_numpy(wl.i2).to(dev))
+    VF = torch.zeros(tuple(reversed((nd,) + wl.vf)), dtype=torch.float64, device=dev)
+    cp = wl.params.to_c()
+    dims = (C.c_int64 * 3)(*(list(shape) + [1] * (3 - nd)))
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
 
     def step():
         rc = ctx.lib.mqp_piv_device(ctx.handle, C.c_void_p(d1.data_ptr()), C.c_void_p(d2.data_ptr()), None, None,
-                                    _lib.MQP_F32, 2, dims, C.byref(cp), C.c_void_p(VF.data_ptr()), None,
+                                    _lib.MQP_F32, nd, dims, C.byref(cp), C.c_void_p(VF.data_ptr()), None,
                                     C.c_void_p(stream.cuda_stream))
         _lib.check(rc, ctx.handle)
 
+    chunk3d = None
+    if nd == 3 and args.chunk3d:
+        chunk3d, tuned = args.chunk3d, "fixed by --chunk3d"
+        ctx.set_chunk3d(chunk3d, 0)
+    elif nd == 3:
+        # launch tuning (results never depend on it): IAs per 3D chunk, timed here
+        chunk3d, tuned = tune.autotune_chunk3d(ctx, step, stream, candidates=(512, 1024, 2048, 4096))
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -237,67 +269,72 @@ def run_ours(args):
     value = world * n_ia * args.steps / (total_ms / 1e3)
 
     # ---- e2e through the public API from pinned host memory ----
-    h1p = torch.empty(H * Wd, dtype=torch.float32, pin_memory=True).numpy().reshape((H, Wd), order="F")
-    h2p = torch.empty(H * Wd, dtype=torch.float32, pin_memory=True).numpy().reshape((H, Wd), order="F")
-    h1p[...] = i1
-    h2p[...] = i2
+    npx = int(np.prod(shape))
+    h1p = torch.empty(npx, dtype=torch.float32, pin_memory=True).numpy().reshape(shape, order="F")
+    h2p = torch.empty(npx, dtype=torch.float32, pin_memory=True).numpy().reshape(shape, order="F")
+    h1p[...] = wl.i1
+    h2p[...] = wl.i2
     for _ in range(max(1, args.warmup // 2)):
-        mq.PIV(h1p, h2p, params, context=ctx)
+        mq.PIV(h1p, h2p, wl.params, context=ctx)
+    e2e_steps = args.steps if nd == 2 else max(3, args.steps // 10)
     e2e_t = []
-    for k in range(args.steps):
+    for k in range(e2e_steps):
         flush.fill_(float(k))
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        VFh, _ = mq.PIV(h1p, h2p, params, context=ctx)
+        VFh, _ = mq.PIV(h1p, h2p, wl.params, context=ctx)
         e2e_t.append(time.perf_counter() - t0)
     e2e_s = sum(e2e_t)
     if world > 1:
         t = torch.tensor([e2e_s], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    e2e_value = world * n_ia * args.steps / e2e_s
+    e2e_value = world * n_ia * e2e_steps / e2e_s
 
     peaks, src = measured_peaks()
     fp32_peak = 148 * 128 * 2 * peaks.get("sm_max_mhz", 1965.0) * 1e6
     kern_ms = prof["ms_piv"] / max(prof["launches_piv"], 1)
-    fl = flops_per_ia(norm=args.alg != "fft") * n_ia
-    achieved = fl / (kern_ms / 1e3)
+    achieved = wl.flop_per_ia * n_ia / (kern_ms / 1e3)
     traffic = None
+    tfile = "piv2d_traffic.json" if nd == 2 else "piv3d_traffic.json"
     try:
-        with open(os.path.join(ROOT, "profiles", "piv2d_traffic.json")) as f:
+        with open(os.path.join(ROOT, "profiles", tfile)) as f:
             tr = json.load(f)
-        # measured DRAM bytes of one launch, scaled by interrogation areas
+        # measured DRAM bytes of one pass, scaled by interrogation areas
         traffic = tr["dram_bytes_per_launch"] * n_ia / tr["ia_per_launch"]
     except Exception:
         pass
-    roof = {"bound": "fp32", "kernel": "piv2d_kernel", "achieved": achieved / 1e12, "peak": fp32_peak / 1e12,
+    kname = "piv2d_kernel" if nd == 2 else "k3a_kernel + k3b_kernel + k3c_kernel (all chunks of one pass)"
+    roof = {"bound": "fp32", "kernel": kname, "achieved": achieved / 1e12, "peak": fp32_peak / 1e12,
             "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": traffic,
-            "traffic_unit": "bytes per launch (ncu dram__bytes_read+write, profiles/piv2d_traffic.json)",
-            "algorithmic_bytes_per_launch": 2 * H * Wd * 4 + (H + 1) * (Wd + 1) * 8 + n_ia * 16,
+            "traffic_unit": f"bytes per pass (ncu dram__bytes_read+write, profiles/{tfile})",
+            "algorithmic_bytes_per_launch": wl.alg_bytes,
             "peak_source": f"148 SM x 128 FP32 lanes x 2 x sm_max_mhz from MEASURED_PEAKS.json ({src})",
-            "kernel_ms": kern_ms, "algorithmic_flop_per_ia": flops_per_ia(norm=args.alg != "fft"),
-            "hbm_frac_of_measured": (2 * H * Wd * 4 + n_ia * 16) / (kern_ms / 1e3) / (peaks.get("hbm_gbs", 6650) * 1e9)}
+            "kernel_ms": kern_ms, "algorithmic_flop_per_ia": wl.flop_per_ia,
+            "hbm_frac_of_measured": wl.alg_bytes / (kern_ms / 1e3) / (peaks.get("hbm_gbs", 6650) * 1e9)}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
-            cpu = cpu_baseline_sample(i1, i2, args)
+            cpu = cpu_baseline_sample(wl)
         except Exception as e:  # reported, never fatal
             cpu = {"value": None, "error": str(e)}
     if rank == 0:
+        cfg = {"workload": wl.desc, "n_ia_per_pair": n_ia, "parallelism": f"replicas x{world}",
+               "l2": "flushed between steps by a 256 MiB write outside the timed events",
+               "compute": "FP32 FFTs, FP64 integral images and normalisation"}
+        if chunk3d:
+            cfg["chunk3d"] = chunk3d
+            cfg["chunk3d_tuning_ms"] = tuned
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": f"vortex pair {args.size}x{args.size} float32, {args.alg}, IS 32 SM 16 step 8",
-                           "n_ia_per_pair": n_ia, "parallelism": f"replicas x{world}",
-                           "l2": "flushed between steps by a 256 MiB write outside the timed events",
-                           "compute": "FP32 FFTs, FP64 integral images and normalisation"},
+                "config": cfg,
                 "e2e": {"value": e2e_value, "unit": UNIT,
-                        "h2d_bytes_per_step": int(2 * H * Wd * 4),
-                        "d2h_bytes_per_step": int(n_ia * 2 * 8)},
-                "gpu_launches": int(prof["launches_piv"] + prof["launches_integral"] * (2 if args.alg != "fft" else 0)
-                                    + (2 * prof["launches_integral"] if args.alg == "zncc" else 0)),
+                        "h2d_bytes_per_step": int(2 * wl.image_bytes),
+                        "d2h_bytes_per_step": int(n_ia * nd * 8)},
+                "gpu_launches": kernel_launches(wl, chunk3d or 1) * args.steps,
                 "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary(),
-                "kernel_ms": {"piv2d": kern_ms, "integral_scans": prof["ms_integral"] / max(args.steps, 1)}}
+                "kernel_ms": {"piv": kern_ms, "integral_scans": prof["ms_integral"] / max(args.steps, 1)}}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
@@ -315,8 +352,10 @@ def main(argv=None):
     ap.add_argument("--size", type=int, default=2048)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ref-budget", type=float, default=10.0)
+    ap.add_argument("--workload", default="vortex2048", choices=["vortex2048", "shear3d"],
+                    help="vortex2048: 2D vortex pair (--size, --alg); shear3d: 512x512x256 FFTCC volumes")
+    ap.add_argument("--chunk3d", type=int, default=0, help="IAs per 3D chunk (0: autotuned in warm-up)")
     args = ap.parse_args(argv)
-    args.n_ia_full = ((args.size - 32) // 8 + 1) ** 2
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

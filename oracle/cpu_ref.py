@@ -85,14 +85,15 @@ def time_sample(i1, i2, alg, budget_s=12.0, IS=32, SM=16, step=8):
     """IA/s of the restatement on all host threads over a bounded prefix of
     the workload's IAs (column-major IA order), sized to ~budget_s."""
     from multi_quickpiv_b200 import setPIVParameters
-    p = setPIVParameters(corr_alg=alg, interSize=(IS, IS), searchMargin=(SM, SM), step=(step, step))
-    p.ndims = i1.ndim
+    nd = i1.ndim
+    p = setPIVParameters(corr_alg=alg, interSize=(IS,) * nd, searchMargin=(SM,) * nd, step=(step,) * nd)
+    p.ndims = nd
     cp = p.to_c()
     nth = threads()
     n_total = 1
     for d in range(i1.ndim):
         n_total *= (i1.shape[d] - IS) // step + 1
-    n = min(n_total, 64 * nth)
+    n = min(n_total, (64 if nd == 2 else 2) * nth)
     t0 = time.perf_counter()
     piv(i1, i2, cp, nthreads=nth, ia_begin=0, ia_end=n)
     dt = time.perf_counter() - t0
