@@ -161,6 +161,81 @@ MQP_API int mqp_profile_read(mqp_ctx* ctx, mqp_profile* out);
 MQP_API int mqp_set_tuning(mqp_ctx* ctx, int key, int64_t value);
 
 /*
+ * Vector-field post-processing: the local-window operations of
+ * src/postprocessing/postprocessing.jl on a Float64 field of `ncomp`
+ * components over an `ndims`-D grid (column-major, component fastest: the
+ * VF array PIV returns; a scalar map has ncomp = 1).  Windows of half-size
+ * `radius` are clamped at the field border as localOp does
+ * (postprocessing.jl:62-72).  Which input/outputs each op uses:
+ *
+ *   op                         replaces (postprocessing.jl)          in      out
+ *   MQP_POST_MAGNITUDES        magnitudes(VF)             :184-192   VF      d_out (dims)
+ *   MQP_POST_AVERAGE           average(radius, VF)        :364-381   VF      d_out (ncomp, dims)
+ *   MQP_POST_SIMILARITY_AVG    similarityAveraging        :475-523   VF      d_out (ncomp, dims)
+ *   MQP_POST_COLLECTIVENESS    collectiveness(radius, VF) :291-331   VF      d_outf (dims, Float32)
+ *   MQP_POST_TH_MASK           TH_masking(th, map; cmp)   :660-670   map     d_mask_out
+ *   MQP_POST_STD_MASK          STD_masking(n, map)        :598-609   map     d_mask_out
+ *   MQP_POST_REPLACE           the replacement step of STD_filtering / TH_filtering /
+ *                              remove_low_SN (:630-643, :692-706, :723-732)
+ *                                                                    VF,mask d_out (ncomp, dims)
+ *   MQP_POST_LOCAL_MAGNITUDE   local_magnitude_mask       :202-218   VF      d_out, d_mask_out (removed)
+ *   MQP_POST_MATLAB_DIVERGENCE matlab_divergence(VF)      :918-941   VF      d_outf (dims, Float32)
+ *   MQP_POST_DIVERGENCE        divergence(radii, VF; ...) :853-903   VF      d_out (dims)
+ *
+ * TH_filtering, remove_low_SN, divergence and the default replaceFun of
+ * STD_filtering cannot run in the reference (see each op's notes in the
+ * library source); these entries compute what they were written to compute.
+ */
+#define MQP_POST_MAGNITUDES 0
+#define MQP_POST_AVERAGE 1
+#define MQP_POST_SIMILARITY_AVG 2
+#define MQP_POST_COLLECTIVENESS 3
+#define MQP_POST_TH_MASK 4
+#define MQP_POST_STD_MASK 5
+#define MQP_POST_REPLACE 6
+#define MQP_POST_LOCAL_MAGNITUDE 7
+#define MQP_POST_MATLAB_DIVERGENCE 8
+#define MQP_POST_DIVERGENCE 9
+
+#define MQP_REPLACE_ZERO 0   /* zeroReplace */
+#define MQP_REPLACE_MEDIAN 1 /* medianReplace */
+#define MQP_REPLACE_MEAN 2   /* meanReplace: the window mean its docstring describes */
+
+#define MQP_DIVIDE_NONE 0
+#define MQP_DIVIDE_N 1       /* divide_by = "N" */
+#define MQP_DIVIDE_MAGS 2    /* divide_by = "mags" */
+
+typedef struct mqp_field {
+  int32_t ncomp;    /* components per vector (1 = scalar map) */
+  int32_t ndims;    /* grid dimensions, 1..4 */
+  int64_t dims[4];  /* grid size (unused entries ignored) */
+} mqp_field;
+
+typedef struct mqp_post_params {
+  int32_t op;                   /* MQP_POST_* */
+  int32_t radius[4];            /* window half-size per grid axis (divergence: the sink radii) */
+  double max_angle;             /* degrees: collectiveness (default 40), similarityAveraging (20) */
+  int32_t normalize;            /* similarityAveraging (default 1), divergence (default 0) */
+  int32_t scale_by_similarity;  /* similarityAveraging (default 1) */
+  double similarity_exponent;   /* similarityAveraging (default 2) */
+  double threshold;             /* TH_MASK: th; STD_MASK: n; LOCAL_MAGNITUDE: ratio */
+  int32_t cmp;                  /* TH_MASK: 0 = (x > th), 1 = (x < th) */
+  int32_t replace;              /* REPLACE: MQP_REPLACE_* */
+  double min_speed;             /* divergence (default 0) */
+  int32_t divide_by;            /* divergence: MQP_DIVIDE_* (default N) */
+  int32_t circle;               /* divergence (default 0) */
+  int32_t reserved[8];
+} mqp_post_params;
+
+/* On device arrays, enqueued on `stream` (NULL = legacy default stream). */
+MQP_API int mqp_postprocess_device(mqp_ctx* ctx, const mqp_post_params* p, const mqp_field* f, const double* d_in,
+                                   const uint8_t* d_mask, double* d_out, float* d_outf, uint8_t* d_mask_out,
+                                   void* stream);
+/* The same on host arrays (copied through the context's device buffers; blocks). */
+MQP_API int mqp_postprocess(mqp_ctx* ctx, const mqp_post_params* p, const mqp_field* f, const double* in,
+                            const uint8_t* mask, double* out, float* outf, uint8_t* mask_out);
+
+/*
  * Allocation-free 2D PIV.  No counterpart in the reference: it exists for
  * callers that cannot allocate GPU memory when they compute a vector field
  * (code running under a framework that owns all device memory through its

@@ -9,6 +9,7 @@ from .piv import (PIV, PIVParameters, _isize, _ovp, _smarg, _ssize, _step,  # no
                   correlation_planes, get_vectorfield_size, maxval, parseCorr,
                   setPIVParameters, toDims3)
 from ._lib import Context, MQPError  # noqa: F401
+from . import postprocessing  # noqa: F401
 
 __all__ = ["PIV", "PIVParameters", "setPIVParameters", "get_vectorfield_size", "correlation_planes",
            "Context", "MQPError", "maxval"]

@@ -62,6 +62,34 @@ class MqpProfile(C.Structure):
     ]
 
 
+class MqpField(C.Structure):
+    _fields_ = [("ncomp", C.c_int32), ("ndims", C.c_int32), ("dims", C.c_int64 * 4)]
+
+
+class MqpPostParams(C.Structure):
+    _fields_ = [
+        ("op", C.c_int32),
+        ("radius", C.c_int32 * 4),
+        ("max_angle", C.c_double),
+        ("normalize", C.c_int32),
+        ("scale_by_similarity", C.c_int32),
+        ("similarity_exponent", C.c_double),
+        ("threshold", C.c_double),
+        ("cmp", C.c_int32),
+        ("replace", C.c_int32),
+        ("min_speed", C.c_double),
+        ("divide_by", C.c_int32),
+        ("circle", C.c_int32),
+        ("reserved", C.c_int32 * 8),
+    ]
+
+
+(MQP_POST_MAGNITUDES, MQP_POST_AVERAGE, MQP_POST_SIMILARITY_AVG, MQP_POST_COLLECTIVENESS, MQP_POST_TH_MASK,
+ MQP_POST_STD_MASK, MQP_POST_REPLACE, MQP_POST_LOCAL_MAGNITUDE, MQP_POST_MATLAB_DIVERGENCE,
+ MQP_POST_DIVERGENCE) = range(10)
+MQP_REPLACE_ZERO, MQP_REPLACE_MEDIAN, MQP_REPLACE_MEAN = 0, 1, 2
+MQP_DIVIDE_NONE, MQP_DIVIDE_N, MQP_DIVIDE_MAGS = 0, 1, 2
+
 SIGNATURES = {
     "mqp_abi_version": (C.c_int, []),
     "mqp_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int]),
@@ -79,6 +107,10 @@ SIGNATURES = {
     "mqp_profile_enable": (C.c_int, [C.c_void_p, C.c_int]),
     "mqp_profile_read": (C.c_int, [C.c_void_p, C.POINTER(MqpProfile)]),
     "mqp_set_tuning": (C.c_int, [C.c_void_p, C.c_int, C.c_int64]),
+    "mqp_postprocess_device": (C.c_int, [C.c_void_p, C.POINTER(MqpPostParams), C.POINTER(MqpField), C.c_void_p,
+                                         C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "mqp_postprocess": (C.c_int, [C.c_void_p, C.POINTER(MqpPostParams), C.POINTER(MqpField), C.c_void_p,
+                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 
 _lib = None

@@ -45,6 +45,7 @@ struct mqp_ctx {
   std::mutex mu;
   DevBuf img1, img2, mask, mask_skip, II1, IIg, IIg2, VF, SN, pred, planes, status, iscratch, scratch3d;
   DevBuf passVF[2];  // vectors of the coarse passes of a multi-pass refinement
+  DevBuf post_in, post_mask, post_out, post_outf, post_mask_out, post_scratch;
   // 3D path: IAs per chunk (0 = sized from chunk3d_budget bytes of scratch)
   int64_t chunk3d = 0;
   size_t chunk3d_budget = (size_t)1 << 30;
@@ -181,7 +182,8 @@ int mqp_destroy(mqp_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (DevBuf* b : {&ctx->img1, &ctx->img2, &ctx->mask, &ctx->mask_skip, &ctx->II1, &ctx->IIg, &ctx->IIg2,
                     &ctx->VF, &ctx->SN, &ctx->pred, &ctx->planes, &ctx->status, &ctx->iscratch,
-                    &ctx->scratch3d, &ctx->passVF[0], &ctx->passVF[1]})
+                    &ctx->scratch3d, &ctx->passVF[0], &ctx->passVF[1], &ctx->post_in, &ctx->post_mask,
+                    &ctx->post_out, &ctx->post_outf, &ctx->post_mask_out, &ctx->post_scratch})
     b->release();
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -592,6 +594,188 @@ int mqp_profile_read(mqp_ctx* ctx, mqp_profile* out) {
   }
   ctx->spans.clear();
   *out = ctx->prof;
+  return MQP_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Validates a post-processing request and fills the kernel arguments.
+int post_resolve(mqp_ctx* ctx, const mqp_post_params* p, const mqp_field* f, mqp::PostArgs& a) {
+  if (!p || !f) return fail(ctx, MQP_ERR_INVALID, "null parameters or field");
+  if (f->ndims < 1 || f->ndims > 4) return fail(ctx, MQP_ERR_INVALID, "field ndims must be 1..4");
+  if (f->ncomp < 1 || f->ncomp > 4) return fail(ctx, MQP_ERR_INVALID, "field ncomp must be 1..4");
+  memset(&a, 0, sizeof(a));
+  a.op = p->op;
+  a.ncomp = f->ncomp;
+  a.nd = f->ndims;
+  a.n = 1;
+  for (int d = 0; d < 4; ++d) {
+    const int64_t n = d < f->ndims ? f->dims[d] : 1;
+    if (n < 0 || n > (1 << 30)) return fail(ctx, MQP_ERR_INVALID, "field extents must be in [0, 2^30]");
+    a.dims[d] = (int)n;
+    a.radius[d] = d < f->ndims ? p->radius[d] : 0;
+    if (a.radius[d] < 0) return fail(ctx, MQP_ERR_INVALID, "radius must be >= 0");
+    a.n *= n;
+  }
+  switch (p->op) {
+    case MQP_POST_MAGNITUDES:
+    case MQP_POST_AVERAGE:
+      break;
+    case MQP_POST_SIMILARITY_AVG:
+      a.p0 = cospi(p->max_angle / 180.0);  // cosd
+      a.i0 = p->normalize != 0;
+      a.i1 = p->scale_by_similarity != 0;
+      a.p1 = p->similarity_exponent;
+      break;
+    case MQP_POST_COLLECTIVENESS:
+      a.p0 = cospi(p->max_angle / 180.0);
+      break;
+    case MQP_POST_TH_MASK:
+      if (f->ncomp != 1) return fail(ctx, MQP_ERR_INVALID, "TH masking takes a scalar map (ncomp = 1)");
+      a.p0 = p->threshold;
+      a.i0 = p->cmp != 0;
+      break;
+    case MQP_POST_STD_MASK:
+      if (f->ncomp != 1) return fail(ctx, MQP_ERR_INVALID, "STD masking takes a scalar map (ncomp = 1)");
+      if (a.n < 2) return fail(ctx, MQP_ERR_INVALID, "STD masking needs at least two values");
+      a.p0 = p->threshold;
+      break;
+    case MQP_POST_REPLACE:
+      if (p->replace < MQP_REPLACE_ZERO || p->replace > MQP_REPLACE_MEAN)
+        return fail(ctx, MQP_ERR_INVALID, "replace must be MQP_REPLACE_ZERO, _MEDIAN or _MEAN");
+      a.i0 = p->replace;
+      break;
+    case MQP_POST_LOCAL_MAGNITUDE:
+      a.p0 = p->threshold;
+      break;
+    case MQP_POST_MATLAB_DIVERGENCE:
+      if (f->ncomp != f->ndims) return fail(ctx, MQP_ERR_INVALID, "matlab_divergence needs ncomp == ndims");
+      break;
+    case MQP_POST_DIVERGENCE:
+      if (f->ncomp != f->ndims) return fail(ctx, MQP_ERR_INVALID, "divergence needs ncomp == ndims");
+      a.i0 = p->normalize != 0;
+      a.p1 = p->min_speed;
+      a.i1 = p->divide_by;
+      a.i2 = p->circle != 0;
+      if (a.i1 < MQP_DIVIDE_NONE || a.i1 > MQP_DIVIDE_MAGS) return fail(ctx, MQP_ERR_INVALID, "bad divide_by");
+      break;
+    default:
+      return fail(ctx, MQP_ERR_INVALID, "unknown post-processing op " + std::to_string(p->op));
+  }
+  return MQP_OK;
+}
+
+// which buffers an op reads/writes: in (ncomp-vector or scalar), mask, out
+// (Float64, vector or scalar), outf (Float32 scalar), mask_out
+struct PostIO {
+  bool mask, out_vec, out_scalar, outf, mask_out;
+};
+PostIO post_io(int op) {
+  switch (op) {
+    case MQP_POST_MAGNITUDES: return {false, false, true, false, false};
+    case MQP_POST_AVERAGE:
+    case MQP_POST_SIMILARITY_AVG: return {false, true, false, false, false};
+    case MQP_POST_COLLECTIVENESS:
+    case MQP_POST_MATLAB_DIVERGENCE: return {false, false, false, true, false};
+    case MQP_POST_TH_MASK:
+    case MQP_POST_STD_MASK: return {false, false, false, false, true};
+    case MQP_POST_REPLACE: return {true, true, false, false, false};
+    case MQP_POST_LOCAL_MAGNITUDE: return {false, true, false, false, true};
+    case MQP_POST_DIVERGENCE: return {false, false, true, false, false};
+    default: return {false, false, false, false, false};
+  }
+}
+
+int post_run(mqp_ctx* ctx, mqp::PostArgs& a, const double* d_in, const uint8_t* d_mask, double* d_out,
+             float* d_outf, uint8_t* d_mask_out, cudaStream_t s) {
+  const PostIO io = post_io(a.op);
+  if (!d_in) return fail(ctx, MQP_ERR_INVALID, "null input field");
+  if ((io.mask && !d_mask) || ((io.out_vec || io.out_scalar) && !d_out) || (io.outf && !d_outf) ||
+      (io.mask_out && !d_mask_out))
+    return fail(ctx, MQP_ERR_INVALID, "a buffer this op needs is null");
+  a.VF = d_in;
+  a.mask = d_mask;
+  a.out = d_out;
+  a.outf = d_outf;
+  a.mask_out = d_mask_out;
+  cudaError_t e;
+  if (a.op == MQP_POST_STD_MASK) {
+    if ((e = ctx->post_scratch.ensure(mqp::post_scratch_bytes())) != cudaSuccess) return cuda_fail(ctx, e, "scratch");
+  }
+  ProfileScope ps(ctx, s, 2, 0);
+  if ((e = mqp::launch_post(a, (double*)ctx->post_scratch.ptr, s)) != cudaSuccess) return cuda_fail(ctx, e, "post-processing kernel");
+  return MQP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mqp_postprocess_device(mqp_ctx* ctx, const mqp_post_params* p, const mqp_field* f, const double* d_in,
+                           const uint8_t* d_mask, double* d_out, float* d_outf, uint8_t* d_mask_out, void* stream) {
+  if (!ctx) return fail(nullptr, MQP_ERR_INVALID, "null context");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  mqp::PostArgs a;
+  int rc = post_resolve(ctx, p, f, a);
+  if (rc != MQP_OK) return rc;
+  return post_run(ctx, a, d_in, d_mask, d_out, d_outf, d_mask_out, stream ? (cudaStream_t)stream : cudaStreamLegacy);
+}
+
+int mqp_postprocess(mqp_ctx* ctx, const mqp_post_params* p, const mqp_field* f, const double* in, const uint8_t* mask,
+                    double* out, float* outf, uint8_t* mask_out) {
+  if (!ctx) return fail(nullptr, MQP_ERR_INVALID, "null context");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  mqp::PostArgs a;
+  int rc = post_resolve(ctx, p, f, a);
+  if (rc != MQP_OK) return rc;
+  if (!in) return fail(ctx, MQP_ERR_INVALID, "null input field");
+  const PostIO io = post_io(a.op);
+  const bool vec_in = !(a.op == MQP_POST_TH_MASK || a.op == MQP_POST_STD_MASK);
+  const size_t n = (size_t)a.n, nb = n ? n : 1;
+  const size_t in_b = nb * (vec_in ? a.ncomp : 1) * sizeof(double);
+  const size_t out_b = nb * (io.out_vec ? a.ncomp : 1) * sizeof(double);
+  cudaStream_t s = ctx->stream;
+  cudaError_t e;
+  if ((e = ctx->post_in.ensure(in_b)) != cudaSuccess) return cuda_fail(ctx, e, "post-processing buffer");
+  if ((e = cudaMemcpyAsync(ctx->post_in.ptr, in, in_b, cudaMemcpyHostToDevice, s)) != cudaSuccess) return cuda_fail(ctx, e, "copy in");
+  uint8_t* dm = nullptr;
+  if (io.mask) {
+    if (!mask) return fail(ctx, MQP_ERR_INVALID, "this op needs a mask");
+    if ((e = ctx->post_mask.ensure(nb)) != cudaSuccess) return cuda_fail(ctx, e, "post-processing buffer");
+    if ((e = cudaMemcpyAsync(ctx->post_mask.ptr, mask, nb, cudaMemcpyHostToDevice, s)) != cudaSuccess) return cuda_fail(ctx, e, "copy mask");
+    dm = (uint8_t*)ctx->post_mask.ptr;
+  }
+  double* dout = nullptr;
+  float* doutf = nullptr;
+  uint8_t* dmo = nullptr;
+  if (io.out_vec || io.out_scalar) {
+    if (!out) return fail(ctx, MQP_ERR_INVALID, "this op needs `out`");
+    if ((e = ctx->post_out.ensure(out_b)) != cudaSuccess) return cuda_fail(ctx, e, "post-processing buffer");
+    dout = (double*)ctx->post_out.ptr;
+  }
+  if (io.outf) {
+    if (!outf) return fail(ctx, MQP_ERR_INVALID, "this op needs `outf`");
+    if ((e = ctx->post_outf.ensure(nb * sizeof(float))) != cudaSuccess) return cuda_fail(ctx, e, "post-processing buffer");
+    doutf = (float*)ctx->post_outf.ptr;
+  }
+  if (io.mask_out) {
+    if (!mask_out) return fail(ctx, MQP_ERR_INVALID, "this op needs `mask_out`");
+    if ((e = ctx->post_mask_out.ensure(nb)) != cudaSuccess) return cuda_fail(ctx, e, "post-processing buffer");
+    dmo = (uint8_t*)ctx->post_mask_out.ptr;
+  }
+  rc = post_run(ctx, a, (const double*)ctx->post_in.ptr, dm, dout, doutf, dmo, s);
+  if (rc != MQP_OK) {
+    cudaStreamSynchronize(s);
+    return rc;
+  }
+  if (n && dout && (e = cudaMemcpyAsync(out, dout, out_b, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return cuda_fail(ctx, e, "copy out");
+  if (n && doutf && (e = cudaMemcpyAsync(outf, doutf, n * sizeof(float), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return cuda_fail(ctx, e, "copy out");
+  if (n && dmo && (e = cudaMemcpyAsync(mask_out, dmo, n, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return cuda_fail(ctx, e, "copy out");
+  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(ctx, e, "post-processing");
   return MQP_OK;
 }
 

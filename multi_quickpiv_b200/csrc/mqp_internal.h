@@ -9,6 +9,7 @@
 #include "mqp_piv2d.cuh"
 #include "mqp_piv3d.cuh"
 #include "mqp_multipass.cuh"
+#include "mqp_post.cuh"
 
 namespace mqp {
 
@@ -45,5 +46,9 @@ cudaError_t launch_piv3d(const Piv3dArgs& a, int alg, long long chunk, cudaStrea
 
 // Multi-pass refinement: the fine pass's predictor from the coarse vectors.
 cudaError_t launch_predictor(const PredArgs& a, cudaStream_t s);
+
+// Vector-field post-processing (one op); scratch holds post_scratch_bytes().
+cudaError_t launch_post(const PostArgs& a, double* scratch, cudaStream_t s);
+size_t post_scratch_bytes();
 
 }  // namespace mqp

@@ -28,21 +28,24 @@ def test_library_exports_every_declared_symbol():
     assert set(syms) <= set(_lib.SIGNATURES), "binding lacks a declared symbol"
 
 
-def test_abi_version_and_struct_layout(tmp_path):
-    """The ctypes mirror of mqp_params matches the C layout (size and every
-    field offset), checked by compiling a probe against include/mqp.h."""
+@pytest.mark.parametrize("cname,py", [("mqp_params", "MqpParams"), ("mqp_profile", "MqpProfile"),
+                                      ("mqp_field", "MqpField"), ("mqp_post_params", "MqpPostParams")])
+def test_abi_version_and_struct_layout(tmp_path, cname, py):
+    """Each ctypes mirror matches the C layout (size and every field offset),
+    checked by compiling a probe against include/mqp.h."""
     import subprocess
     lib = _lib.load()
     assert lib.mqp_abi_version() == 1
-    fields = [f for f, _ in _lib.MqpParams._fields_]
+    st = getattr(_lib, py)
+    fields = [f for f, _ in st._fields_]
     src = tmp_path / "probe.c"
-    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "mqp.h"\nint main(void){printf("%zu", sizeof(mqp_params));' +
-                   "".join(f'printf(" %zu", offsetof(mqp_params, {f}));' for f in fields) + "return 0;}\n")
+    src.write_text(f'#include <stdio.h>\n#include <stddef.h>\n#include "mqp.h"\nint main(void){{printf("%zu", sizeof({cname}));' +
+                   "".join(f'printf(" %zu", offsetof({cname}, {f}));' for f in fields) + "return 0;}\n")
     exe = tmp_path / "probe"
     subprocess.run(["gcc", "-I", os.path.dirname(HEADER), str(src), "-o", str(exe)], check=True)
     got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
-    assert got[0] == C.sizeof(_lib.MqpParams)
-    assert got[1:] == [getattr(_lib.MqpParams, f).offset for f in fields]
+    assert got[0] == C.sizeof(st)
+    assert got[1:] == [getattr(st, f).offset for f in fields]
 
 
 def test_vf_dims_matches_reference_formula():
