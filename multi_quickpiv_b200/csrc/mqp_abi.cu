@@ -11,146 +11,10 @@
 #include <vector>
 
 #include "mqp.h"
+#include "mqp_ctx.h"
 #include "mqp_internal.h"
 
-namespace {
-
-thread_local std::string g_create_error;
-
-struct DevBuf {
-  void* ptr = nullptr;
-  size_t bytes = 0;
-  cudaError_t ensure(size_t n) {
-    if (n <= bytes) return cudaSuccess;
-    if (ptr) cudaFree(ptr);
-    ptr = nullptr;
-    bytes = 0;
-    cudaError_t e = cudaMalloc(&ptr, n);
-    if (e == cudaSuccess) bytes = n;
-    return e;
-  }
-  void release() {
-    if (ptr) cudaFree(ptr);
-    ptr = nullptr;
-    bytes = 0;
-  }
-};
-
-}  // namespace
-
-struct mqp_ctx {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  std::string last_error;
-  std::mutex mu;
-  DevBuf img1, img2, mask, mask_skip, II1, IIg, IIg2, VF, SN, pred, planes, status, iscratch, scratch3d;
-  DevBuf passVF[2];  // vectors of the coarse passes of a multi-pass refinement
-  DevBuf post_in, post_mask, post_out, post_outf, post_mask_out, post_scratch;
-  // 3D path: IAs per chunk (0 = sized from chunk3d_budget bytes of scratch)
-  int64_t chunk3d = 0;
-  size_t chunk3d_budget = (size_t)1 << 30;
-  // tracing
-  bool profile = false;
-  struct Span {
-    cudaEvent_t a, b;
-    int kind;  // 0 integral, 1 piv, 2 other
-    int64_t ia;
-  };
-  std::vector<Span> spans;
-  mqp_profile prof{};
-};
-
-namespace {
-
-struct ProfileScope {
-  mqp_ctx* ctx;
-  cudaStream_t s;
-  mqp_ctx::Span sp{};
-  bool on;
-  ProfileScope(mqp_ctx* c, cudaStream_t st, int kind, int64_t ia) : ctx(c), s(st), on(c->profile) {
-    if (!on) return;
-    sp.kind = kind;
-    sp.ia = ia;
-    cudaEventCreate(&sp.a);
-    cudaEventCreate(&sp.b);
-    cudaEventRecord(sp.a, s);
-  }
-  ~ProfileScope() {
-    if (!on) return;
-    cudaEventRecord(sp.b, s);
-    ctx->spans.push_back(sp);
-  }
-};
-
-}  // namespace
-
-namespace {
-
-// A resolved single-pass problem: per-axis sizes after toDims3 / _isize /
-// _smarg / _step (src/piv_parameters.jl:83-87).
-struct Problem {
-  int ndims = 2;
-  int64_t dims[3] = {1, 1, 1};
-  int IS[3] = {0, 0, 0}, SM[3] = {0, 0, 0}, st[3] = {1, 1, 1};
-  int64_t vf[3] = {1, 1, 1};
-  int64_t n_ia = 0;
-  int alg = 2;
-};
-
-int fail(mqp_ctx* ctx, int code, const std::string& msg) {
-  if (ctx) ctx->last_error = msg;
-  else g_create_error = msg;
-  return code;
-}
-
-int cuda_fail(mqp_ctx* ctx, cudaError_t e, const char* what) {
-  const int code = (e == cudaErrorMemoryAllocation) ? MQP_ERR_OOM : MQP_ERR_CUDA;
-  return fail(ctx, code, std::string(what) + ": " + cudaGetErrorString(e));
-}
-
-// get_vectorfield_size (src/utils/piv_ops.jl:11-14)
-int64_t vf_len(int64_t size, int IS, int st) {
-  const int64_t stop = size - IS + 1;
-  return stop < 1 ? 0 : (stop - 1) / st + 1;
-}
-
-int resolve(mqp_ctx* ctx, const mqp_params* p, int ndims, const int64_t dims[3], bool masked,
-            int scale, Problem& pb) {
-  if (!p || !dims) return fail(ctx, MQP_ERR_INVALID, "null parameter or dims pointer");
-  if (ndims != 2 && ndims != 3) return fail(ctx, MQP_ERR_INVALID, "ndims must be 2 or 3");
-  // gaussian_displacement's padded branch is a broken path in the reference
-  // (src/utils/piv_ops.jl:261-266 prints ERROR and indexes out of range)
-  if (!p->unpadded)
-    return fail(ctx, MQP_ERR_UNSUPPORTED,
-                "ERROR: all gaussian_displacement should be unpadded (stored unpadded must be true; "
-                "setPIVParameters stores the good_pad argument there)");
-  if (p->multipass < 1) return fail(ctx, MQP_ERR_INVALID, "multipass must be >= 1");
-  pb.ndims = ndims;
-  pb.alg = masked ? mqp::ALG_MASK_NSQECC : p->corr_alg;
-  if (!masked && (p->corr_alg < 0 || p->corr_alg > 2))
-    return fail(ctx, MQP_ERR_INVALID, "corr_alg must be MQP_FFTCC, MQP_ZNCC or MQP_NSQECC");
-  pb.n_ia = 1;
-  for (int d = 0; d < 3; ++d) {
-    pb.dims[d] = d < ndims ? dims[d] : 1;
-    if (d >= ndims) {
-      pb.vf[d] = 1;
-      continue;
-    }
-    if (dims[d] < 1) return fail(ctx, MQP_ERR_INVALID, "image extents must be >= 1");
-    if (dims[d] > (int64_t)1 << 30) return fail(ctx, MQP_ERR_INVALID, "image extent too large");
-    pb.IS[d] = p->interSize[d] * scale;
-    pb.SM[d] = p->searchMargin[d] * scale;
-    pb.st[d] = p->has_step ? p->step[d] * scale : pb.IS[d] - p->overlap[d] * scale;
-    if (pb.IS[d] < 1) return fail(ctx, MQP_ERR_INVALID, "interSize must be >= 1 along every image axis");
-    if (pb.SM[d] < 0) return fail(ctx, MQP_ERR_INVALID, "searchMargin must be >= 0");
-    if (pb.st[d] < 1) return fail(ctx, MQP_ERR_INVALID, "step (or interSize - overlap) must be >= 1");
-    pb.vf[d] = vf_len(dims[d], pb.IS[d], pb.st[d]);
-    pb.n_ia *= pb.vf[d];
-  }
-  return MQP_OK;
-}
-
-}  // namespace
+using namespace mqp_host;
 
 extern "C" {
 
@@ -208,7 +72,7 @@ int mqp_vf_dims(const mqp_params* p, int ndims, const int64_t dims[3], int64_t v
 
 }  // extern "C"
 
-namespace {
+namespace mqp_host {
 
 size_t elem_size(int dtype) { return dtype == MQP_F64 ? 8 : 4; }
 
@@ -461,7 +325,7 @@ int piv_device_impl(mqp_ctx* ctx, const void* d1, const void* d2, const void* dm
   return run_pass_2d(ctx, pb, p, d1, d2, dmask, dmask_skip, dtype, dVF, dSN, nullptr, dplanes, ia_begin, ia_end, s);
 }
 
-}  // namespace
+}  // namespace mqp_host
 
 extern "C" {
 

@@ -36,6 +36,29 @@ cudaError_t launch_piv2d(const Piv2dArgs& a, int alg, cudaStream_t s, std::strin
 
 int device_sm_count(int device);
 
+// One persistent launch of the fused 2D kernel over the IAs of many image
+// pairs that share a kernel variant (N, prune, alg, dtype): items[k] (device
+// array) is pair k's arguments, prefix[k] the first work-queue index of its
+// IAs (n_items + 1 entries, prefix[n_items] = total).  wf2 is the per-warp
+// workspace (piv2d_warp_f2) of the largest lag plane among the items;
+// counter is one device word the launch resets and uses as the queue head;
+// grab is the queue entries a warp takes at once.
+struct Piv2dBatch {
+  const Piv2dArgs* items;
+  const long long* prefix;
+  int n_items;
+  long long total;
+  int N;
+  bool prune;
+  int alg;
+  int dtype;
+  int wf2;
+  int grab;
+  unsigned long long* counter;
+};
+int piv2d_warp_f2(int N, bool prune, int P1, int P2, bool masked);
+cudaError_t launch_piv2d_batch(const Piv2dBatch& b, cudaStream_t s, std::string& err);
+
 // 3D path: cubic FFT length for the search window (0 = unsupported), chunk
 // scratch bytes per IA, and the three-kernel launch over [a.ia_begin,
 // a.ia_end) in chunks of `chunk` IAs (the scratch pointers of `a` must hold

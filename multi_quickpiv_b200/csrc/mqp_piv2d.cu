@@ -205,6 +205,208 @@ __device__ __forceinline__ void warp_peak(double& best, int& bidx) {
 // ---------------------------------------------------------------------------
 // the fused kernel
 // ---------------------------------------------------------------------------
+// One interrogation area, the whole per-IA body of PIV_CPU's loop, for one
+// warp.  GH is the warp's shared-memory workspace (Layout2d, sized for this
+// IA's lag plane), tw the (cos, sin)(2 pi j / N) table.
+template <int N, bool FPRUNE, int ALG, typename T>
+__device__ __forceinline__ void piv2d_ia(const Piv2dArgs& a, long long ia, float2* GH, const float2* tw, int lane) {
+  using Lay = Layout2d<N, FPRUNE>;
+  constexpr int M = N / 2;
+  constexpr bool MASKED = ALG == ALG_MASK_NSQECC;
+  const int P1 = 2 * a.SM1 + 1, P2 = 2 * a.SM2 + 1;
+  float2* FH = GH + Lay::F_OFF;
+  double* plane = reinterpret_cast<double*>(FH);
+  float* c1buf = MASKED ? reinterpret_cast<float*>(FH + Lay::region2_f2(P1, P2)) : nullptr;
+  const double scale = cc_scale<N>();
+  // lag rows [0, lane_rows) go one per lane; a short tail of rows
+  // (2*SM1+1 just above 32) is computed by the whole warp, lanes over s2
+  const int lane_rows = (P1 - 32 > 0 && P1 - 32 <= 4) ? 32 : P1;
+  const int v1 = (int)(ia % a.vf1), v2 = (int)(ia / a.vf1);
+  int d1, d2;
+  ia_pred(a, v1, v2, d1, d2);
+  const IAGeom g = ia_geom(a, v1, v2);
+  IAScalars sc;
+  sc.meanF = 0.0;
+  sc.meanG = 0.0;
+  if (ALG == ALG_ZNCC) {
+    // copy_*_minus_mean! (src/utils/zncc_ops.jl:7-25): IA mean and the mean
+    // of the whole clipped search region
+    sc.meanF = box_sum(a.II1, a.H, g.ir1, g.ir1 + a.IS1, g.ir2, g.ir2 + a.IS2) / ((double)a.IS1 * a.IS2);
+    const double nG = (double)(g.hi1 - g.lo1) * (double)(g.hi2 - g.lo2);
+    sc.meanG = box_sum(a.IIg, a.H, g.g01 + g.lo1, g.g01 + g.hi1, g.g02 + g.lo2, g.g02 + g.hi2) / nG;
+  }
+  const long long vfo = (long long)v1 + (long long)a.vf1 * v2;
+  bool skipped = false;
+
+  // One pass correlates one pair of inputs; masked NSQECC needs two
+  // ((F*mask) with G, mask with G^2, mask_nsqecc.jl:151-155).
+  constexpr int NPASS = MASKED ? 2 : 1;
+#pragma unroll 1
+  for (int pass = 0; pass < NPASS; ++pass) {
+    const int pmode = MASKED ? (pass == 0 ? PASS_MASKED : PASS_MASK_SQ) : PASS_PLAIN;
+
+    // ---- phase 1: F rows and G rows, r2c along dim 2 (one rolled body) ----
+    // The loads of the next row are in flight while the current row is
+    // transformed.
+    constexpr int NJF = (Lay::NF + 31) / 32, NJ = NJF + N / 32;
+    double vmax = -INFINITY, mmax = -INFINITY, sumsq = 0.0;
+    float buf[N];
+    RowJob jn = row_job<N, FPRUNE>(a, g, lane, 0);
+    row_load<N, T>(a, jn, buf);
+#pragma unroll 1
+    for (int job = 0; job < NJ; ++job) {
+      const RowJob jc = jn;
+      float cur[N];
+#pragma unroll
+      for (int x = 0; x < N; ++x) cur[x] = buf[x];
+      if (job + 1 < NJ) {
+        jn = row_job<N, FPRUNE>(a, g, lane, job + 1);
+        row_load<N, T>(a, jn, buf);
+      }
+      if (!(jc.isF && jc.row >= Lay::NF))
+        row_process<N, FPRUNE, T, ALG == ALG_ZNCC>(a, sc, pmode, jc, cur, GH, FH, vmax, mmax, sumsq);
+    }
+    if (pass == 0) {
+      vmax = warp_max(vmax);
+      sc.sumF2 = warp_sum(sumsq);
+      // skip_inter_region (src/utils/piv_ops.jl:134-157): the vector stays zero
+      bool skip;
+      if (MASKED) {
+        mmax = warp_max(mmax);
+        skip = (a.threshold > 0.0 && vmax < a.threshold) || (a.mask_threshold > 0.0 && mmax < a.mask_threshold);
+      } else {
+        skip = a.threshold >= 0.0 && vmax < a.threshold;
+      }
+      if (skip) {
+        skipped = true;
+        break;
+      }
+    }
+    __syncwarp();
+#pragma unroll 1
+    for (int n = lane; n < M; n += 32) split_G_pair<N, FPRUNE>(GH, tw, n);
+    __syncwarp();
+
+    // ---- phases 2 and 3: one rolled loop of stages around one FFT body ----
+    // The plane is row-contiguous: element (s1, s2) at s1*P2 + s2.
+    {
+      constexpr int RU = (M + 31) / 32;  // spectrum rows per lane
+      const int NS2 = 6 * RU;            // phase-2 stages
+      const int RL = (lane_rows + 31) / 32;
+      float2 t[M];  // carried from the F stage (the product) into the I stage
+#pragma unroll 1
+      for (int job = 0; job < NS2 + RL; ++job) {
+        if (job == NS2) __syncwarp();  // all spectra rows finished before phase 3
+        bool active;
+        int st = 0, h = 0, u = 0, s1 = 0;
+        if (job < NS2) {
+          const int q = job % 6;
+          u = lane + 32 * (job / 6);
+          h = q / 3;
+          st = q % 3;
+          active = u < M;
+          if (active) stage_pre<N, FPRUNE>(st, h, GH + u * Lay::GSTR, FH + u * Lay::FSTR, t);
+        } else {
+          s1 = lane + 32 * (job - NS2);
+          active = s1 < lane_rows;
+          if (active) c2r_pre<N, FPRUNE>(s1, GH, t);
+        }
+        if (!active) continue;
+        fft_reg<M, false>(t);
+        if (job < NS2) {
+          stage_post<N, FPRUNE>(st, h, u == 0, P1, GH + u * Lay::GSTR, t);
+        } else {
+          double* prow = plane + s1 * P2;
+#pragma unroll
+          for (int n = 0; n < M; ++n) {
+            const float2 z = cconj(t[fpos<M>(n)]);
+            if (2 * n < P2) prow[2 * n] = (double)z.x * scale;
+            if (2 * n + 1 < P2) prow[2 * n + 1] = (double)z.y * scale;
+          }
+        }
+      }
+    }
+    __syncwarp();
+    // raw correlation of the tail lag rows, all lanes over s2
+#pragma unroll 1
+    for (int s1 = lane_rows; s1 < P1; ++s1)
+      for (int s2 = lane; s2 < P2; s2 += 32)
+        plane[s1 * P2 + s2] = (double)tail_row_value<N, FPRUNE>(GH, tw, s1, s2) * scale;
+    __syncwarp();
+    if (MASKED && pass == 0) {
+      // park (F*mask)*G while the second pass reuses the workspace
+      for (int i = lane; i < P1 * P2; i += 32) c1buf[i] = (float)plane[i];
+      __syncwarp();
+    }
+  }
+  if (skipped) {
+    if (lane == 0) {
+      a.VF[2 * vfo + 0] = 0.0;
+      a.VF[2 * vfo + 1] = 0.0;
+      if (a.SN) a.SN[vfo] = 0.0;
+    }
+    if (a.planes) {
+      double* dst = a.planes + (ia - a.ia_begin) * (long long)P1 * P2;
+      for (int i = lane; i < P1 * P2; i += 32) dst[i] = 0.0;
+    }
+    __syncwarp();
+    return;
+  }
+
+  // ---- finish: similarity, peak (first_fullovp_peak), SN, Gaussian fit ----
+  LagRanges R;
+  R.lo1 = g.tlf1;
+  R.hi1 = 2 * a.SM1 - g.brb1;
+  R.lo2 = g.tlf2;
+  R.hi2 = 2 * a.SM2 - g.brb2;
+  R.shi1 = 2 * a.SM1 - 1 - g.brb1;
+  R.shi2 = 2 * a.SM2 - 1 - g.brb2;
+  PeakAcc acc;
+  acc.best = 0.0;
+  acc.bidx = -1;
+  acc.smax = -INFINITY;
+  acc.ssum = 0.0;
+#pragma unroll 1
+  for (int s1 = lane; s1 < lane_rows; s1 += 32)
+    finish_row<ALG>(a, g, sc, s1, P1, P2, plane + s1 * P2, R, acc, MASKED ? c1buf + s1 * P2 : nullptr);
+#pragma unroll 1
+  for (int s1 = lane_rows; s1 < P1; ++s1)
+    for (int s2 = lane; s2 < P2; s2 += 32) {
+      double& e = plane[s1 * P2 + s2];
+      e = finish_one<ALG>(a, g, sc, s1, s2, e, MASKED ? (double)c1buf[s1 * P2 + s2] : 0.0);
+      acc_take(acc, R, s1, s2, P1, e);
+    }
+  __syncwarp();
+  double best = acc.best;
+  int bidx = acc.bidx;
+  warp_peak(best, bidx);
+  double sn = 0.0;
+  if (a.SN) {
+    // compute_SN (src/utils/piv_ops.jl:336-367) over [TLF_off, 2SM-1-BRB_off]
+    const double smax = warp_nmax(acc.smax);
+    const double ssum = warp_sum(acc.ssum);
+    const double len = (double)(R.shi1 - R.lo1 + 1) * (double)(R.shi2 - R.lo2 + 1);
+    sn = smax / ((ssum - smax) / (len - 1.0));
+  }
+  if (a.planes) {
+    double* dst = a.planes + (ia - a.ia_begin) * (long long)P1 * P2;
+    for (int i = lane; i < P1 * P2; i += 32) dst[i] = plane[(i % P1) * P2 + i / P1];
+  }
+  if (lane == 0) {
+    double r1, r2;
+    if (bidx < 0) {
+      r1 = -1.0;  // 1-based peak (0, 0): displacement -(SM+1)
+      r2 = -1.0;
+    } else {
+      refine2d(plane, P2, a.SM1, a.SM2, g, bidx % P1, bidx / P1, best, r1, r2);
+    }
+    a.VF[2 * vfo + 0] = r1 - a.SM1 + d1;
+    a.VF[2 * vfo + 1] = r2 - a.SM2 + d2;
+    if (a.SN) a.SN[vfo] = sn;
+  }
+  __syncwarp();
+}
+
 // Persistent: each warp walks IAs ia = first + k * (all warps).  The warp's
 // shared-memory workspace holds the spectra rows of G (N/2 x (N+1)) and F
 // (N/2 x (NF+1)); after phase 2 the F rows are reused for the FP64 plane.
@@ -212,209 +414,51 @@ template <int N, bool FPRUNE, int ALG, typename T, int WARPS, int MINB>
 __global__ void __launch_bounds__(WARPS * 32, MINB) piv2d_kernel(Piv2dArgs a) {
   extern __shared__ float2 smem[];
   using Lay = Layout2d<N, FPRUNE>;
-  constexpr int M = N / 2;
   constexpr bool MASKED = ALG == ALG_MASK_NSQECC;
   const int P1 = 2 * a.SM1 + 1, P2 = 2 * a.SM2 + 1;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wf2 = Lay::warp_f2(P1, P2, MASKED);
   float2* GH = smem + (size_t)warp * wf2;
-  float2* FH = GH + Lay::F_OFF;
-  double* plane = reinterpret_cast<double*>(FH);
-  float* c1buf = MASKED ? reinterpret_cast<float*>(FH + Lay::region2_f2(P1, P2)) : nullptr;
   float2* tw = smem + (size_t)WARPS * wf2;  // (cos, sin)(2 pi j / N)
   for (int j = threadIdx.x; j < N; j += blockDim.x) tw[j] = twiddle_cs(j * (TW_N / N));
   __syncthreads();
   const long long nwarps = (long long)gridDim.x * WARPS;
-  const double scale = cc_scale<N>();
-  // lag rows [0, lane_rows) go one per lane; a short tail of rows
-  // (2*SM1+1 just above 32) is computed by the whole warp, lanes over s2
-  const int lane_rows = (P1 - 32 > 0 && P1 - 32 <= 4) ? 32 : P1;
+  for (long long ia = a.ia_begin + (long long)blockIdx.x * WARPS + warp; ia < a.ia_end; ia += nwarps)
+    piv2d_ia<N, FPRUNE, ALG, T>(a, ia, GH, tw, lane);
+}
 
-  for (long long ia = a.ia_begin + (long long)blockIdx.x * WARPS + warp; ia < a.ia_end; ia += nwarps) {
-    const int v1 = (int)(ia % a.vf1), v2 = (int)(ia / a.vf1);
-    int d1, d2;
-    ia_pred(a, v1, v2, d1, d2);
-    const IAGeom g = ia_geom(a, v1, v2);
-    IAScalars sc;
-    sc.meanF = 0.0;
-    sc.meanG = 0.0;
-    if (ALG == ALG_ZNCC) {
-      // copy_*_minus_mean! (src/utils/zncc_ops.jl:7-25): IA mean and the mean
-      // of the whole clipped search region
-      sc.meanF = box_sum(a.II1, a.H, g.ir1, g.ir1 + a.IS1, g.ir2, g.ir2 + a.IS2) / ((double)a.IS1 * a.IS2);
-      const double nG = (double)(g.hi1 - g.lo1) * (double)(g.hi2 - g.lo2);
-      sc.meanG = box_sum(a.IIg, a.H, g.g01 + g.lo1, g.g01 + g.hi1, g.g02 + g.lo2, g.g02 + g.hi2) / nG;
+// Batched: the IAs of many image pairs sharing one kernel variant form one
+// work queue [0, total); prefix[k] is the first queue index of item k
+// (prefix[n_items] = total).  Warps take `grab` consecutive queue entries at
+// a time from `counter` (zeroed before the launch), so large and small pairs
+// balance across the SMs.  wf2: float2 per warp, the largest any item needs.
+template <int N, bool FPRUNE, int ALG, typename T, int WARPS, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB)
+    piv2d_batch_kernel(const Piv2dArgs* __restrict__ items, const long long* __restrict__ prefix, int n_items,
+                       long long total, int wf2, int grab, unsigned long long* counter) {
+  extern __shared__ float2 smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float2* GH = smem + (size_t)warp * wf2;
+  float2* tw = smem + (size_t)WARPS * wf2;
+  for (int j = threadIdx.x; j < N; j += blockDim.x) tw[j] = twiddle_cs(j * (TW_N / N));
+  __syncthreads();
+  for (;;) {
+    unsigned long long g0 = 0;
+    if (lane == 0) g0 = atomicAdd(counter, (unsigned long long)grab);
+    g0 = __shfl_sync(0xffffffffu, g0, 0);
+    if ((long long)g0 >= total) break;
+    for (int t = 0; t < grab; ++t) {
+      const long long gi = (long long)g0 + t;
+      if (gi >= total) break;
+      int lo = 0, hi = n_items - 1;  // last k with prefix[k] <= gi
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (prefix[mid] <= gi) lo = mid;
+        else hi = mid - 1;
+      }
+      const Piv2dArgs& a = items[lo];
+      piv2d_ia<N, FPRUNE, ALG, T>(a, a.ia_begin + (gi - prefix[lo]), GH, tw, lane);
     }
-    const long long vfo = (long long)v1 + (long long)a.vf1 * v2;
-    bool skipped = false;
-
-    // One pass correlates one pair of inputs; masked NSQECC needs two
-    // ((F*mask) with G, mask with G^2, mask_nsqecc.jl:151-155).
-    constexpr int NPASS = MASKED ? 2 : 1;
-#pragma unroll 1
-    for (int pass = 0; pass < NPASS; ++pass) {
-      const int pmode = MASKED ? (pass == 0 ? PASS_MASKED : PASS_MASK_SQ) : PASS_PLAIN;
-
-      // ---- phase 1: F rows and G rows, r2c along dim 2 (one rolled body) ----
-      // The loads of the next row are in flight while the current row is
-      // transformed.
-      constexpr int NJF = (Lay::NF + 31) / 32, NJ = NJF + N / 32;
-      double vmax = -INFINITY, mmax = -INFINITY, sumsq = 0.0;
-      float buf[N];
-      RowJob jn = row_job<N, FPRUNE>(a, g, lane, 0);
-      row_load<N, T>(a, jn, buf);
-#pragma unroll 1
-      for (int job = 0; job < NJ; ++job) {
-        const RowJob jc = jn;
-        float cur[N];
-#pragma unroll
-        for (int x = 0; x < N; ++x) cur[x] = buf[x];
-        if (job + 1 < NJ) {
-          jn = row_job<N, FPRUNE>(a, g, lane, job + 1);
-          row_load<N, T>(a, jn, buf);
-        }
-        if (!(jc.isF && jc.row >= Lay::NF))
-          row_process<N, FPRUNE, T, ALG == ALG_ZNCC>(a, sc, pmode, jc, cur, GH, FH, vmax, mmax, sumsq);
-      }
-      if (pass == 0) {
-        vmax = warp_max(vmax);
-        sc.sumF2 = warp_sum(sumsq);
-        // skip_inter_region (src/utils/piv_ops.jl:134-157): the vector stays zero
-        bool skip;
-        if (MASKED) {
-          mmax = warp_max(mmax);
-          skip = (a.threshold > 0.0 && vmax < a.threshold) || (a.mask_threshold > 0.0 && mmax < a.mask_threshold);
-        } else {
-          skip = a.threshold >= 0.0 && vmax < a.threshold;
-        }
-        if (skip) {
-          skipped = true;
-          break;
-        }
-      }
-      __syncwarp();
-#pragma unroll 1
-      for (int n = lane; n < M; n += 32) split_G_pair<N, FPRUNE>(GH, tw, n);
-      __syncwarp();
-
-      // ---- phases 2 and 3: one rolled loop of stages around one FFT body ----
-      // The plane is row-contiguous: element (s1, s2) at s1*P2 + s2.
-      {
-        constexpr int RU = (M + 31) / 32;  // spectrum rows per lane
-        const int NS2 = 6 * RU;            // phase-2 stages
-        const int RL = (lane_rows + 31) / 32;
-        float2 t[M];  // carried from the F stage (the product) into the I stage
-#pragma unroll 1
-        for (int job = 0; job < NS2 + RL; ++job) {
-          if (job == NS2) __syncwarp();  // all spectra rows finished before phase 3
-          bool active;
-          int st = 0, h = 0, u = 0, s1 = 0;
-          if (job < NS2) {
-            const int q = job % 6;
-            u = lane + 32 * (job / 6);
-            h = q / 3;
-            st = q % 3;
-            active = u < M;
-            if (active) stage_pre<N, FPRUNE>(st, h, GH + u * Lay::GSTR, FH + u * Lay::FSTR, t);
-          } else {
-            s1 = lane + 32 * (job - NS2);
-            active = s1 < lane_rows;
-            if (active) c2r_pre<N, FPRUNE>(s1, GH, t);
-          }
-          if (!active) continue;
-          fft_reg<M, false>(t);
-          if (job < NS2) {
-            stage_post<N, FPRUNE>(st, h, u == 0, P1, GH + u * Lay::GSTR, t);
-          } else {
-            double* prow = plane + s1 * P2;
-#pragma unroll
-            for (int n = 0; n < M; ++n) {
-              const float2 z = cconj(t[fpos<M>(n)]);
-              if (2 * n < P2) prow[2 * n] = (double)z.x * scale;
-              if (2 * n + 1 < P2) prow[2 * n + 1] = (double)z.y * scale;
-            }
-          }
-        }
-      }
-      __syncwarp();
-      // raw correlation of the tail lag rows, all lanes over s2
-#pragma unroll 1
-      for (int s1 = lane_rows; s1 < P1; ++s1)
-        for (int s2 = lane; s2 < P2; s2 += 32)
-          plane[s1 * P2 + s2] = (double)tail_row_value<N, FPRUNE>(GH, tw, s1, s2) * scale;
-      __syncwarp();
-      if (MASKED && pass == 0) {
-        // park (F*mask)*G while the second pass reuses the workspace
-        for (int i = lane; i < P1 * P2; i += 32) c1buf[i] = (float)plane[i];
-        __syncwarp();
-      }
-    }
-    if (skipped) {
-      if (lane == 0) {
-        a.VF[2 * vfo + 0] = 0.0;
-        a.VF[2 * vfo + 1] = 0.0;
-        if (a.SN) a.SN[vfo] = 0.0;
-      }
-      if (a.planes) {
-        double* dst = a.planes + (ia - a.ia_begin) * (long long)P1 * P2;
-        for (int i = lane; i < P1 * P2; i += 32) dst[i] = 0.0;
-      }
-      __syncwarp();
-      continue;
-    }
-
-    // ---- finish: similarity, peak (first_fullovp_peak), SN, Gaussian fit ----
-    LagRanges R;
-    R.lo1 = g.tlf1;
-    R.hi1 = 2 * a.SM1 - g.brb1;
-    R.lo2 = g.tlf2;
-    R.hi2 = 2 * a.SM2 - g.brb2;
-    R.shi1 = 2 * a.SM1 - 1 - g.brb1;
-    R.shi2 = 2 * a.SM2 - 1 - g.brb2;
-    PeakAcc acc;
-    acc.best = 0.0;
-    acc.bidx = -1;
-    acc.smax = -INFINITY;
-    acc.ssum = 0.0;
-#pragma unroll 1
-    for (int s1 = lane; s1 < lane_rows; s1 += 32)
-      finish_row<ALG>(a, g, sc, s1, P1, P2, plane + s1 * P2, R, acc, MASKED ? c1buf + s1 * P2 : nullptr);
-#pragma unroll 1
-    for (int s1 = lane_rows; s1 < P1; ++s1)
-      for (int s2 = lane; s2 < P2; s2 += 32) {
-        double& e = plane[s1 * P2 + s2];
-        e = finish_one<ALG>(a, g, sc, s1, s2, e, MASKED ? (double)c1buf[s1 * P2 + s2] : 0.0);
-        acc_take(acc, R, s1, s2, P1, e);
-      }
-    __syncwarp();
-    double best = acc.best;
-    int bidx = acc.bidx;
-    warp_peak(best, bidx);
-    double sn = 0.0;
-    if (a.SN) {
-      // compute_SN (src/utils/piv_ops.jl:336-367) over [TLF_off, 2SM-1-BRB_off]
-      const double smax = warp_nmax(acc.smax);
-      const double ssum = warp_sum(acc.ssum);
-      const double len = (double)(R.shi1 - R.lo1 + 1) * (double)(R.shi2 - R.lo2 + 1);
-      sn = smax / ((ssum - smax) / (len - 1.0));
-    }
-    if (a.planes) {
-      double* dst = a.planes + (ia - a.ia_begin) * (long long)P1 * P2;
-      for (int i = lane; i < P1 * P2; i += 32) dst[i] = plane[(i % P1) * P2 + i / P1];
-    }
-    if (lane == 0) {
-      double r1, r2;
-      if (bidx < 0) {
-        r1 = -1.0;  // 1-based peak (0, 0): displacement -(SM+1)
-        r2 = -1.0;
-      } else {
-        refine2d(plane, P2, a.SM1, a.SM2, g, bidx % P1, bidx / P1, best, r1, r2);
-      }
-      a.VF[2 * vfo + 0] = r1 - a.SM1 + d1;
-      a.VF[2 * vfo + 1] = r2 - a.SM2 + d2;
-      if (a.SN) a.SN[vfo] = sn;
-    }
-    __syncwarp();
   }
 }
 
@@ -480,6 +524,67 @@ template <int N, bool FPRUNE, int WARPS, int MINB>
 static cudaError_t launch_dt(const Piv2dArgs& a, int alg, cudaStream_t s, std::string& err) {
   return a.dtype == 0 ? launch_alg<N, FPRUNE, float, WARPS, MINB>(a, alg, s, err)
                       : launch_alg<N, FPRUNE, double, WARPS, MINB>(a, alg, s, err);
+}
+
+int piv2d_warp_f2(int N, bool prune, int P1, int P2, bool masked) {
+  if (N == 64) return prune ? Layout2d<64, true>::warp_f2(P1, P2, masked) : Layout2d<64, false>::warp_f2(P1, P2, masked);
+  if (N == 32) return prune ? Layout2d<32, true>::warp_f2(P1, P2, masked) : Layout2d<32, false>::warp_f2(P1, P2, masked);
+  return 0;
+}
+
+template <int N, bool FPRUNE, int ALG, typename T, int WARPS, int MINB>
+static cudaError_t launch_batch_t(const Piv2dBatch& b, cudaStream_t s, std::string& err) {
+  const size_t smem = ((size_t)WARPS * b.wf2 + N) * sizeof(float2);
+  auto kern = piv2d_batch_kernel<N, FPRUNE, ALG, T, WARPS, MINB>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) {
+    err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e);
+    return e;
+  }
+  int dev = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, WARPS * 32, smem);
+  if (e != cudaSuccess || per_sm < 1) {
+    err = "piv2d batch kernel does not fit on an SM (shared memory " + std::to_string(smem) + " B)";
+    return e != cudaSuccess ? e : cudaErrorInvalidConfiguration;
+  }
+  long long blocks = (long long)device_sm_count(dev) * per_sm;
+  const long long need = (b.total + WARPS - 1) / WARPS;
+  if (blocks > need) blocks = need;
+  if (blocks < 1) return cudaSuccess;
+  if ((e = cudaMemsetAsync(b.counter, 0, sizeof(unsigned long long), s)) != cudaSuccess) {
+    err = std::string("counter reset: ") + cudaGetErrorString(e);
+    return e;
+  }
+  kern<<<(unsigned)blocks, WARPS * 32, smem, s>>>(b.items, b.prefix, b.n_items, b.total, b.wf2,
+                                                   b.grab > 0 ? b.grab : 1, b.counter);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) err = std::string("piv2d batch launch: ") + cudaGetErrorString(e);
+  return e;
+}
+
+template <int N, bool FPRUNE, typename T>
+static cudaError_t launch_batch_alg(const Piv2dBatch& b, cudaStream_t s, std::string& err) {
+  switch (b.alg) {
+    case ALG_FFTCC: return launch_batch_t<N, FPRUNE, ALG_FFTCC, T, 4, 2>(b, s, err);
+    case ALG_ZNCC: return launch_batch_t<N, FPRUNE, ALG_ZNCC, T, 4, 2>(b, s, err);
+    case ALG_NSQECC: return launch_batch_t<N, FPRUNE, ALG_NSQECC, T, 4, 2>(b, s, err);
+    case ALG_MASK_NSQECC: return launch_batch_t<N, FPRUNE, ALG_MASK_NSQECC, T, 3, 2>(b, s, err);
+    default: err = "unknown correlation algorithm"; return cudaErrorInvalidValue;
+  }
+}
+
+template <int N, bool FPRUNE>
+static cudaError_t launch_batch_dt(const Piv2dBatch& b, cudaStream_t s, std::string& err) {
+  return b.dtype == 0 ? launch_batch_alg<N, FPRUNE, float>(b, s, err) : launch_batch_alg<N, FPRUNE, double>(b, s, err);
+}
+
+cudaError_t launch_piv2d_batch(const Piv2dBatch& b, cudaStream_t s, std::string& err) {
+  if (b.total <= 0 || b.n_items <= 0) return cudaSuccess;
+  if (b.N == 64) return b.prune ? launch_batch_dt<64, true>(b, s, err) : launch_batch_dt<64, false>(b, s, err);
+  if (b.N == 32) return b.prune ? launch_batch_dt<32, true>(b, s, err) : launch_batch_dt<32, false>(b, s, err);
+  err = "search window larger than 64 along some axis is not supported by the 2D kernel";
+  return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_piv2d(const Piv2dArgs& a, int alg, cudaStream_t s, std::string& err) {

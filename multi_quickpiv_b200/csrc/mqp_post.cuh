@@ -73,12 +73,29 @@ MQP_HD MQP_FI long long post_lin(const PostArgs& a, int i0, int i1, int i2, int 
                                                                                        (long long)a.dims[2] * i3));
 }
 
+// Products and sums rounded separately, as Julia's broadcast-then-sum
+// (`sum(x .^ 2)`, `sum(a .* b)`) rounds them: no fused multiply-add.
+MQP_HD MQP_FI double pmul(double a, double b) {
+#if defined(__CUDA_ARCH__)
+  return __dmul_rn(a, b);
+#else
+  return a * b;
+#endif
+}
+MQP_HD MQP_FI double padd(double a, double b) {
+#if defined(__CUDA_ARCH__)
+  return __dadd_rn(a, b);
+#else
+  return a + b;
+#endif
+}
+
 // magnitudes (postprocessing.jl:184-192): sqrt(sum(VF[:, i].^2))
 MQP_HD MQP_FI double post_mag(const double* VF, int ncomp, long long i) {
   double s = 0.0;
   for (int c = 0; c < ncomp; ++c) {
     const double v = VF[(long long)ncomp * i + c];
-    s += v * v;
+    s = padd(s, pmul(v, v));
   }
   return sqrt(s);
 }
@@ -165,7 +182,7 @@ MQP_HD MQP_FI void post_collectiveness_at(const PostArgs& a, long long i) {
           const double mag_ = post_mag(a.VF, a.ncomp, l);
           double dot = 0.0;
           for (int k = 0; k < a.ncomp; ++k)
-            dot += (a.VF[(long long)a.ncomp * i + k] / mag) * (a.VF[(long long)a.ncomp * l + k] / mag_);
+            dot = padd(dot, pmul(a.VF[(long long)a.ncomp * i + k] / mag, a.VF[(long long)a.ncomp * l + k] / mag_));
           similar += dot > a.p0;
         }
   a.outf[i] = (float)((double)similar / (double)post_count(lo, hi));
@@ -197,16 +214,17 @@ MQP_HD MQP_FI void post_similarity_averaging_at(const PostArgs& a, long long i) 
           const long long l = post_lin(a, w0, w1, w2, w3);
           const double mag_ = post_mag(a.VF, nc, l);
           double dot = 0.0;
-          for (int k = 0; k < nc; ++k) dot += (a.VF[(long long)nc * i + k] / mag) * (a.VF[(long long)nc * l + k] / mag_);
+          for (int k = 0; k < nc; ++k)
+            dot = padd(dot, pmul(a.VF[(long long)nc * i + k] / mag, a.VF[(long long)nc * l + k] / mag_));
           if (dot > a.p0) {
-            for (int k = 0; k < nc && k < 4; ++k) avg[k] += (a.VF[(long long)nc * l + k] / mag_) * mag_;
+            for (int k = 0; k < nc && k < 4; ++k) avg[k] = padd(avg[k], pmul(a.VF[(long long)nc * l + k] / mag_, mag_));
             ++similar;
           }
         }
   double fac = 1.0;
   if (a.i0) {
     double s = 0.0;
-    for (int k = 0; k < nc && k < 4; ++k) s += avg[k] * avg[k];
+    for (int k = 0; k < nc && k < 4; ++k) s = padd(s, pmul(avg[k], avg[k]));
     fac /= sqrt(s);
   }
   if (a.i1) fac *= pow((double)similar / (double)post_count(lo, hi), a.p1);
@@ -304,7 +322,7 @@ MQP_HD MQP_FI double sink_magnitude(const PostArgs& a, const int (&k)[POST_MAXD]
   bool centre = true;
   for (int d = 0; d < a.nd; ++d) {
     const double t = (double)(a.radius[d] - k[d]);
-    s += t * t;
+    s = padd(s, pmul(t, t));
     rmax = a.radius[d] > rmax ? a.radius[d] : rmax;
     centre = centre && k[d] == a.radius[d];
   }
@@ -361,7 +379,7 @@ MQP_HD MQP_FI void post_divergence_at(const PostArgs& a, long long i) {
             double s = 0.0;
             for (int q = 0; q < a.ncomp; ++q) {
               const double v = post_vfnorm(a, l, q);
-              s += v * v;
+              s = padd(s, pmul(v, v));
             }
             smags += sqrt(s);
           }
@@ -369,7 +387,7 @@ MQP_HD MQP_FI void post_divergence_at(const PostArgs& a, long long i) {
           for (int q = 0; q < a.ncomp && q < a.nd; ++q) {
             double sv = (double)(a.radius[q] - k[q]) / sm;
             if (sv != sv) sv = 0.0;
-            acc += sv * post_vfnorm(a, l, q);
+            acc = padd(acc, pmul(sv, post_vfnorm(a, l, q)));
           }
         }
   if (a.i1 == DIVIDE_N) acc /= nsink;
