@@ -161,6 +161,48 @@ MQP_API int mqp_profile_read(mqp_ctx* ctx, mqp_profile* out);
 MQP_API int mqp_set_tuning(mqp_ctx* ctx, int key, int64_t value);
 
 /*
+ * Batched PIV plans.  No counterpart in the reference (whose PIV takes one
+ * pair): many image pairs of mixed size, dimensionality (2D/3D), algorithm,
+ * mask and pass count on DEVICE arrays, computed by one pre-allocated
+ * schedule captured into a CUDA graph.  Every pair's VF/SN equal what
+ * mqp_piv_device returns for it alone.
+ *
+ * The plan keeps the device pointers of the items (and owns all scratch):
+ * run it as often as wanted while they stay valid; results are written to
+ * the items' VF/SN.  Creating a plan allocates and synchronises; running
+ * it enqueues one graph launch on `stream` and returns.
+ */
+typedef struct mqp_batch_item {
+  const void* img1;       /* device images, column-major, dims[0] fastest */
+  const void* img2;
+  const void* mask;       /* masked NSQECC mask (device) or NULL */
+  const void* mask_skip;  /* double-masked skip mask (device) or NULL */
+  int32_t dtype;          /* MQP_F32 / MQP_F64 */
+  int32_t ndims;          /* 2 or 3 */
+  int64_t dims[3];
+  mqp_params params;      /* refine + multipass > 1 gives a multi-pass pair */
+  double* VF;             /* device (ndims, vf...) */
+  double* SN;             /* device (vf...) or NULL */
+} mqp_batch_item;
+
+typedef struct mqp_batch_options {
+  int32_t use_graph;       /* capture the schedule into one CUDA graph (default 1) */
+  int32_t grab;            /* 2D work-queue entries a warp takes at once (default 2) */
+  int64_t chunk3d;         /* IAs per 3D chunk (0 = from chunk3d_budget) */
+  int64_t chunk3d_budget;  /* device bytes of 3D chunk scratch (0 = 1 GiB) */
+  int32_t reserved[8];
+} mqp_batch_options;
+
+typedef struct mqp_plan mqp_plan;
+
+MQP_API int mqp_batch_plan_create(mqp_ctx* ctx, const mqp_batch_item* items, int32_t n_items,
+                                  const mqp_batch_options* opt /* NULL = defaults */, mqp_plan** out);
+MQP_API int mqp_batch_plan_run(mqp_plan* plan, void* stream);
+/* IAs of all passes, kernel launches and scratch bytes of one run */
+MQP_API int mqp_batch_plan_info(const mqp_plan* plan, int64_t* total_ia, int64_t* launches, int64_t* scratch_bytes);
+MQP_API int mqp_batch_plan_destroy(mqp_plan* plan);
+
+/*
  * Vector-field post-processing: the local-window operations of
  * src/postprocessing/postprocessing.jl on a Float64 field of `ncomp`
  * components over an `ndims`-D grid (column-major, component fastest: the

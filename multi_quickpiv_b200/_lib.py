@@ -62,6 +62,20 @@ class MqpProfile(C.Structure):
     ]
 
 
+class MqpBatchItem(C.Structure):
+    _fields_ = [
+        ("img1", C.c_void_p), ("img2", C.c_void_p), ("mask", C.c_void_p), ("mask_skip", C.c_void_p),
+        ("dtype", C.c_int32), ("ndims", C.c_int32), ("dims", C.c_int64 * 3),
+        ("params", MqpParams),
+        ("VF", C.c_void_p), ("SN", C.c_void_p),
+    ]
+
+
+class MqpBatchOptions(C.Structure):
+    _fields_ = [("use_graph", C.c_int32), ("grab", C.c_int32), ("chunk3d", C.c_int64),
+                ("chunk3d_budget", C.c_int64), ("reserved", C.c_int32 * 8)]
+
+
 class MqpField(C.Structure):
     _fields_ = [("ncomp", C.c_int32), ("ndims", C.c_int32), ("dims", C.c_int64 * 4)]
 
@@ -107,6 +121,11 @@ SIGNATURES = {
     "mqp_profile_enable": (C.c_int, [C.c_void_p, C.c_int]),
     "mqp_profile_read": (C.c_int, [C.c_void_p, C.POINTER(MqpProfile)]),
     "mqp_set_tuning": (C.c_int, [C.c_void_p, C.c_int, C.c_int64]),
+    "mqp_batch_plan_create": (C.c_int, [C.c_void_p, C.POINTER(MqpBatchItem), C.c_int32, C.POINTER(MqpBatchOptions),
+                                        C.POINTER(C.c_void_p)]),
+    "mqp_batch_plan_run": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "mqp_batch_plan_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "mqp_batch_plan_destroy": (C.c_int, [C.c_void_p]),
     "mqp_postprocess_device": (C.c_int, [C.c_void_p, C.POINTER(MqpPostParams), C.POINTER(MqpField), C.c_void_p,
                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "mqp_postprocess": (C.c_int, [C.c_void_p, C.POINTER(MqpPostParams), C.POINTER(MqpField), C.c_void_p,

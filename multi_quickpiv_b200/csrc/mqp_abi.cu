@@ -83,7 +83,7 @@ int run_pass_2d(mqp_ctx* ctx, const Problem& pb, const mqp_params* p, const void
   const int H = (int)pb.dims[0], W = (int)pb.dims[1];
   const int SS1 = pb.IS[0] + 2 * pb.SM[0], SS2 = pb.IS[1] + 2 * pb.SM[1];
   if (mqp::piv2d_fft_len(SS1, SS2) == 0)
-    return fail(ctx, MQP_ERR_UNSUPPORTED, "2D search window (interSize + 2 searchMargin) above 64 is not supported yet");
+    return fail(ctx, MQP_ERR_UNSUPPORTED, "2D search window (interSize + 2 searchMargin) above 128 is not supported");
   if (pb.IS[0] > H || pb.IS[1] > W) return MQP_OK;  // empty vector field
   const size_t ii_bytes = (size_t)(H + 1) * (size_t)(W + 1) * sizeof(double);
   cudaError_t e;

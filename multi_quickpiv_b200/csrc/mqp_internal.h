@@ -26,8 +26,8 @@ cudaError_t launch_integral3d(const void* img, int dtype, int H, int W, int D, b
                               double* out, double* scratch, cudaStream_t s);
 size_t integral3d_scratch_bytes(int H, int W, int D);
 
-// Smallest supported power-of-two FFT length covering the search window,
-// or 0 when the window is too large for the fused 2D kernel.
+// Smallest supported power-of-two FFT length covering the search window
+// (32, 64: the warp kernel; 128: the block kernel), or 0 when too large.
 int piv2d_fft_len(int SS1, int SS2);
 
 // Launch the fused 2D kernel over [a.ia_begin, a.ia_end).  `alg` picks the
@@ -58,6 +58,13 @@ struct Piv2dBatch {
 };
 int piv2d_warp_f2(int N, bool prune, int P1, int P2, bool masked);
 cudaError_t launch_piv2d_batch(const Piv2dBatch& b, cudaStream_t s, std::string& err);
+
+// Search windows 65..128 (FFT length 128): one 128-thread block per IA
+// (mqp_piv2d_big.cu); for these, Piv2dBatch::wf2 is the block's whole
+// workspace (piv2d_warp_f2 with N = 128).
+int piv2d_big_warp_f2(bool prune, int P1, int P2, bool masked);
+cudaError_t launch_piv2d_big(const Piv2dArgs& a, int alg, cudaStream_t s, std::string& err);
+cudaError_t launch_piv2d_big_batch(const Piv2dBatch& b, cudaStream_t s, std::string& err);
 
 // 3D path: cubic FFT length for the search window (0 = unsupported), chunk
 // scratch bytes per IA, and the three-kernel launch over [a.ia_begin,

@@ -76,7 +76,7 @@ extern "C" int mqp_piv2d_noalloc(const void* d_img1, const void* d_img2, int dty
     vf[d] = stop < 1 ? 0 : (stop - 1) / st[d] + 1;
   }
   if (mqp::piv2d_fft_len(IS[0] + 2 * SM[0], IS[1] + 2 * SM[1]) == 0)
-    return report(err, errlen, MQP_ERR_UNSUPPORTED, "2D search window (interSize + 2 searchMargin) above 64");
+    return report(err, errlen, MQP_ERR_UNSUPPORTED, "2D search window (interSize + 2 searchMargin) above 128");
   if (vf[0] * vf[1] == 0) return MQP_OK;
 
   // scratch plan: [II of img2^2 | II of img2 | II of img1 | scan totals]

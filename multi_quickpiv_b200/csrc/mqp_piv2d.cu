@@ -469,6 +469,7 @@ int piv2d_fft_len(int SS1, int SS2) {
   const int SS = SS1 > SS2 ? SS1 : SS2;
   if (SS <= 32) return 32;
   if (SS <= 64) return 64;
+  if (SS <= 128) return 128;  // block kernel, mqp_piv2d_big.cu
   return 0;
 }
 
@@ -527,6 +528,7 @@ static cudaError_t launch_dt(const Piv2dArgs& a, int alg, cudaStream_t s, std::s
 }
 
 int piv2d_warp_f2(int N, bool prune, int P1, int P2, bool masked) {
+  if (N == 128) return piv2d_big_warp_f2(prune, P1, P2, masked);
   if (N == 64) return prune ? Layout2d<64, true>::warp_f2(P1, P2, masked) : Layout2d<64, false>::warp_f2(P1, P2, masked);
   if (N == 32) return prune ? Layout2d<32, true>::warp_f2(P1, P2, masked) : Layout2d<32, false>::warp_f2(P1, P2, masked);
   return 0;
@@ -581,6 +583,7 @@ static cudaError_t launch_batch_dt(const Piv2dBatch& b, cudaStream_t s, std::str
 
 cudaError_t launch_piv2d_batch(const Piv2dBatch& b, cudaStream_t s, std::string& err) {
   if (b.total <= 0 || b.n_items <= 0) return cudaSuccess;
+  if (b.N == 128) return launch_piv2d_big_batch(b, s, err);
   if (b.N == 64) return b.prune ? launch_batch_dt<64, true>(b, s, err) : launch_batch_dt<64, false>(b, s, err);
   if (b.N == 32) return b.prune ? launch_batch_dt<32, true>(b, s, err) : launch_batch_dt<32, false>(b, s, err);
   err = "search window larger than 64 along some axis is not supported by the 2D kernel";
@@ -593,7 +596,8 @@ cudaError_t launch_piv2d(const Piv2dArgs& a, int alg, cudaStream_t s, std::strin
   const bool prune = (a.IS1 <= N / 2) && (a.IS2 <= N / 2);
   if (N == 64) return prune ? launch_dt<64, true, 4, 2>(a, alg, s, err) : launch_dt<64, false, 4, 2>(a, alg, s, err);
   if (N == 32) return prune ? launch_dt<32, true, 4, 2>(a, alg, s, err) : launch_dt<32, false, 4, 2>(a, alg, s, err);
-  err = "search window larger than 64 along some axis is not supported by the 2D kernel";
+  if (N == 128) return launch_piv2d_big(a, alg, s, err);
+  err = "search window larger than 128 along some axis is not supported by the 2D kernels";
   return cudaErrorInvalidValue;
 }
 

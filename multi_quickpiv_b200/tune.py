@@ -38,3 +38,27 @@ def autotune_chunk3d(ctx, step: Callable[[], None], stream,
     best = min(res, key=res.get)
     ctx.set_chunk3d(best, 0)
     return best, res
+
+
+def autotune_batch(pairs, candidates=None, context=None, reps: int = 2):
+    """Builds the batch plan of `pairs` with each candidate option set
+    (dicts of mqp_batch_options fields), times one run of each by CUDA events
+    and returns (best options, {str(options): ms}, the best plan)."""
+    import torch
+
+    from .batch import BatchPlan
+    if candidates is None:
+        candidates = [dict(grab=g, use_graph=1, chunk3d=c) for g in (1, 2, 4) for c in (0, 2048)]
+    res = {}
+    best = None
+    for opt in candidates:
+        plan = BatchPlan(pairs, opt, context)
+        ms = time_ms(plan.run, torch.cuda.current_stream(plan.device), reps)
+        res[str(opt)] = ms
+        if best is None or ms < best[1]:
+            if best is not None:
+                best[2].close()
+            best = (opt, ms, plan)
+        else:
+            plan.close()
+    return best[0], res, best[2]

@@ -29,7 +29,8 @@ def test_library_exports_every_declared_symbol():
 
 
 @pytest.mark.parametrize("cname,py", [("mqp_params", "MqpParams"), ("mqp_profile", "MqpProfile"),
-                                      ("mqp_field", "MqpField"), ("mqp_post_params", "MqpPostParams")])
+                                      ("mqp_field", "MqpField"), ("mqp_post_params", "MqpPostParams"),
+                                      ("mqp_batch_item", "MqpBatchItem"), ("mqp_batch_options", "MqpBatchOptions")])
 def test_abi_version_and_struct_layout(tmp_path, cname, py):
     """Each ctypes mirror matches the C layout (size and every field offset),
     checked by compiling a probe against include/mqp.h."""

@@ -113,3 +113,40 @@ def test_emulated_masked_skip(emu):
     VF, SN, _ = run_emu(emu, i1, i2, "nsqecc", (32, 32), (16, 16), (16, 16), mask=mask, mask_skip=skipm, mthr=0.5)
     assert np.all(VF[:, 0, 0] == 0) and np.all(VFo[:, 0, 0] == 0)
     assert np.max(np.abs(VF - VFo)) < 1e-3
+
+
+BIG = [((64, 64), (32, 32), (32, 32)), ((40, 48), (30, 24), (20, 24)), ((72, 40), (20, 30), (24, 20)),
+       ((64, 32), (32, 40), (32, 24))]
+
+
+@pytest.mark.parametrize("alg", ["fft", "zncc", "nsqecc"])
+@pytest.mark.parametrize("cfg", BIG, ids=["is64", "aniso", "unpruned", "wide_sm"])
+def test_emulated_big_window_matches_oracle(emu, alg, cfg):
+    """Search windows 65..128: the 128-thread block kernel's phases."""
+    IS, SM, st = cfg
+    i1, i2, _ = synth.pair_2d_shift(shape=(232, 216), shift=(9.3, -12.6), seed_stream=23)
+    i1, i2 = i1.astype(np.float32), i2.astype(np.float32)
+    po = O.set_piv_parameters(corr_alg=alg, interSize=IS, searchMargin=SM, step=st, computeSN=True)
+    po.ndims = 2
+    VFo, SNo, Co = O.piv_single_pass(i1, i2, po, keep_corr=True)
+    VF, SN, PL = run_emu(emu, i1, i2, alg, IS, SM, st)
+    worst, near_tie = compare_planes(PL, Co, i1.shape, IS, SM, st)
+    assert worst <= PLANE_RTOL, worst
+    bad = (np.abs(VF - VFo) > VF_ATOL).any(axis=0) & ~near_tie
+    assert not bad.any(), np.abs(VF - VFo).max()
+    assert (sn_ok(SN, SNo) | near_tie).all()
+
+
+def test_emulated_big_window_masked(emu):
+    IS, SM, st = (64, 64), (32, 32), (32, 32)
+    i1, i2, _ = synth.pair_2d_shift(shape=(224, 224), shift=(7.2, 5.4), seed_stream=24)
+    mask = synth.ellipse_mask(np.random.default_rng(9), i1.shape, cover=0.7)
+    po = O.set_piv_parameters(interSize=IS, searchMargin=SM, step=st, computeSN=True)
+    po.ndims = 2
+    VFo, SNo, Co = O.piv_single_pass(i1, i2, po, mask=mask, keep_corr=True)
+    VF, SN, PL = run_emu(emu, i1, i2, "nsqecc", IS, SM, st, mask=mask)
+    sparse = mask_coverage(mask, i1.shape, IS, st) < 0.25
+    worst, near_tie = compare_planes(PL, Co, i1.shape, IS, SM, st, skip=sparse)
+    assert worst <= MASK_PLANE_RTOL, worst
+    bad = (np.abs(VF - VFo) > VF_ATOL).any(axis=0) & ~near_tie
+    assert not bad.any(), np.abs(VF - VFo).max()

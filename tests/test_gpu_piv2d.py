@@ -111,3 +111,29 @@ def test_double_masked_skip(gpu):
     VFo, SNo = O.piv_single_pass(i1, i2, po, mask=mask_ia, mask_skip=mask_vf)
     assert np.all(VF[:, 0, 0] == 0) and np.all(VFo[:, 0, 0] == 0)
     assert np.nanmax(np.abs(VF - VFo)) < VF_ATOL
+
+
+@pytest.mark.parametrize("alg", ["fft", "zncc", "nsqecc"])
+@pytest.mark.parametrize("cfg", [((64, 64), (32, 32), (32, 32)), ((40, 48), (30, 24), (20, 24)),
+                                 ((72, 40), (20, 30), (24, 20))], ids=["is64", "aniso", "unpruned"])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_piv2d_big_window_matches_oracle(alg, cfg, dtype, gpu):
+    """Search windows 65..128 run on the 128-thread block kernel."""
+    i1, i2, _ = synth.pair_2d_shift(shape=(264, 248), shift=(9.3, -12.6), seed_stream=25)
+    _compare(i1.astype(dtype), i2.astype(dtype), alg, *cfg)
+
+
+def test_piv2d_big_window_masked(gpu):
+    IS, SM, st = (64, 64), (32, 32), (32, 32)
+    i1, i2, _ = synth.pair_2d_shift(shape=(224, 224), shift=(7.2, 5.4), seed_stream=24)
+    mask = synth.ellipse_mask(np.random.default_rng(9), i1.shape, cover=0.7)
+    po = _oracle_params("nsqecc", IS, SM, st)
+    VFo, SNo, Co = O.piv_single_pass(i1, i2, po, mask=mask, keep_corr=True)
+    pp = setPIVParameters(interSize=IS, searchMargin=SM, step=st, computeSN=True)
+    VF, SN = PIV(i1, i2, mask, pp)
+    planes = correlation_planes(i1, i2, pp, mask=mask)
+    sparse = mask_coverage(mask, i1.shape, IS, st) < 0.25
+    worst, near_tie = compare_planes(planes, Co, i1.shape, IS, SM, st, skip=sparse)
+    assert worst <= MASK_PLANE_RTOL, worst
+    bad = (np.abs(VF - VFo) > VF_ATOL).any(axis=0) & ~near_tie
+    assert not bad.any(), np.abs(VF - VFo).max()
