@@ -30,7 +30,8 @@ __device__ __forceinline__ double bwarp_nmax(double v) {
 }
 
 // One IA; every thread of the block takes part.  sm: the block's workspace
-// (LayBig, sized for this IA's lag plane), red: 16 doubles of scratch.
+// (LayBig, sized for this IA's lag plane), red: its last LayBig::RED_F2 slots
+// (16 doubles: four per warp for the block reductions).
 template <bool FPRUNE, int ALG, typename T>
 __device__ __forceinline__ void piv2d_big_ia(const Piv2dArgs& a, long long ia, float2* sm, double* red) {
   using L = LayBig<FPRUNE>;
@@ -168,11 +169,11 @@ __device__ __forceinline__ void piv2d_big_ia(const Piv2dArgs& a, long long ia, f
 }
 
 // Persistent over the IAs of one pair; wsz = the block's workspace (float2),
-// whose last 8 slots are the reduction scratch.
+// whose last LayBig::RED_F2 slots are the reduction scratch.
 template <bool FPRUNE, int ALG, typename T>
 __global__ void __launch_bounds__(BIG_THREADS) piv2d_big_kernel(Piv2dArgs a, int wsz) {
   extern __shared__ float2 smem[];
-  double* red = reinterpret_cast<double*>(smem + wsz - 8);
+  double* red = reinterpret_cast<double*>(smem + wsz - LayBig<FPRUNE>::RED_F2);
   for (long long ia = a.ia_begin + blockIdx.x; ia < a.ia_end; ia += gridDim.x) piv2d_big_ia<FPRUNE, ALG, T>(a, ia, smem, red);
 }
 
@@ -183,7 +184,7 @@ __global__ void __launch_bounds__(BIG_THREADS)
     piv2d_big_batch_kernel(const Piv2dArgs* __restrict__ items, const long long* __restrict__ prefix, int n_items,
                            long long total, int wsz, int grab, unsigned long long* counter) {
   extern __shared__ float2 smem[];
-  double* red = reinterpret_cast<double*>(smem + wsz - 8);
+  double* red = reinterpret_cast<double*>(smem + wsz - LayBig<FPRUNE>::RED_F2);
   __shared__ unsigned long long g0s;
   for (;;) {
     if (threadIdx.x == 0) g0s = atomicAdd(counter, (unsigned long long)grab);

@@ -53,9 +53,10 @@ struct LayBig {
   static MQP_HD MQP_FI int region2(int P1, int P2) { return F_SIZE > P1 * P2 ? F_SIZE : P1 * P2; }
   static MQP_HD MQP_FI int extra(bool masked, int P1, int P2) { return masked ? (P1 * P2 + 1) / 2 : 0; }
   // after the plane (and the parked masked correlation): the packed column's
-  // F bins (2 x 64) and 8 slots of block reduction
+  // F bins (2 x 64) and RED_F2 slots (16 doubles) of block reduction
+  static constexpr int RED_F2 = 16;
   static MQP_HD MQP_FI int pk_off(int P1, int P2, bool masked) { return S_SIZE + region2(P1, P2) + extra(masked, P1, P2); }
-  static MQP_HD MQP_FI int total_f2(int P1, int P2, bool masked) { return pk_off(P1, P2, masked) + 2 * MB + 8; }
+  static MQP_HD MQP_FI int total_f2(int P1, int P2, bool masked) { return pk_off(P1, P2, masked) + 2 * MB + RED_F2; }
 };
 
 // ---- rows -------------------------------------------------------------------
@@ -213,36 +214,34 @@ MQP_HD MQP_FI void big_col_park_a(int t, const float2 (&p)[MB], float2* S) {
   big_col_park<FPRUNE>(t, p, S);
 }
 
-// Step 5 (after the pair parked both halves): recombine.  Lane h = 0 keeps
-// lags s < min(P1, 64) in out[s]; lane h = 1 keeps lag 64 (when P1 > 64) in
-// out[0].
+// Step 5 (after the pair parked both halves): recombine.  Lane h keeps the
+// lags 64h + s < P1 in out[s]: x[s] = A0[s] + W^-s A1[s] (h = 0) and
+// x[s + 64] = A0[s] - W^-s A1[s] (h = 1).
 template <bool FPRUNE>
 MQP_HD MQP_FI void big_col_combine(int t, int P1, const float2* S, float2 (&out)[MB]) {
   using L = LayBig<FPRUNE>;
   const int c = t >> 1, h = t & 1;
   const float2* row = S + c * L::SSTR;
-  if (h == 0) {
+  const int n = P1 - MB * h;  // lags this lane keeps
 #pragma unroll
-    for (int s = 0; s < MB; ++s)
-      if (s < P1) out[s] = cadd(row[s], rotate<NB, true>(row[MB + s], s));
-  } else if (P1 > MB) {
-    out[0] = csub(row[0], row[MB]);
+  for (int s = 0; s < MB; ++s) {
+    if (s < n) {
+      const float2 w = rotate<NB, true>(row[MB + s], s);
+      out[s] = h ? csub(row[s], w) : cadd(row[s], w);
+    }
   }
 }
 
 // Step 6 (after every lane finished with S): lag rows s1 < P1 of column c into
-// T[s1][c] (T aliases S).
+// T[s1][c] (T aliases S; P1 <= 127 rows of TSTR fit in the G spectra area).
 template <bool FPRUNE>
 MQP_HD MQP_FI void big_col_store(int t, int P1, const float2 (&out)[MB], float2* T) {
   using L = LayBig<FPRUNE>;
   const int c = t >> 1, h = t & 1;
-  if (h == 0) {
+  const int n = P1 - MB * h;
 #pragma unroll
-    for (int s = 0; s < MB; ++s)
-      if (s < P1) T[s * L::TSTR + c] = out[s];
-  } else if (P1 > MB) {
-    T[MB * L::TSTR + c] = out[0];
-  }
+  for (int s = 0; s < MB; ++s)
+    if (s < n) T[(MB * h + s) * L::TSTR + c] = out[s];
 }
 
 #if defined(__CUDACC__)

@@ -206,6 +206,7 @@ int piv3d_fft_len(const int SS[3]) {
   if (SS[2] > m) m = SS[2];
   if (m <= 32) return 32;
   if (m <= 64) return 64;
+  if (m <= 128) return 128;  // only with every interSize <= 64 (launch_piv3d)
   return 0;
 }
 
@@ -240,7 +241,10 @@ cudaError_t launch_piv3d(const Piv3dArgs& a, int alg, long long chunk, cudaStrea
   const bool prune = piv3d_prune(a.IS, N);
   if (N == 64) return prune ? run_dt<64, true>(a, alg, chunk, s, err) : run_dt<64, false>(a, alg, chunk, s, err);
   if (N == 32) return prune ? run_dt<32, true>(a, alg, chunk, s, err) : run_dt<32, false>(a, alg, chunk, s, err);
-  err = "3D search window (interSize + 2 searchMargin) above 64 along some axis is not supported";
+  // search windows 65..128 (the coarse passes of interSize-64 refinements):
+  // the same kernels at length 128, for interrogation windows up to 64
+  if (N == 128 && prune) return run_dt<128, true>(a, alg, chunk, s, err);
+  err = "3D search window (interSize + 2 searchMargin) above 128, or above 64 with an interSize above 64, is not supported";
   return cudaErrorInvalidValue;
 }
 

@@ -172,8 +172,9 @@ extern "C" __attribute__((visibility("default"))) int mqp_emu_piv3d(
   a.ia_end = ia_end;
   a.threshold = threshold;
   a.mask_threshold = mask_threshold;
-  const int N = SS <= 32 ? 32 : (SS <= 64 ? 64 : 0);
+  const int N = SS <= 32 ? 32 : (SS <= 64 ? 64 : (SS <= 128 ? 128 : 0));
   const bool prune = IS[0] <= N / 2 && IS[1] <= N / 2 && IS[2] <= N / 2;
+  if (N == 128) return prune ? emu3_alg<128, true>(a, alg) : -2;
   if (N == 64) return prune ? emu3_alg<64, true>(a, alg) : emu3_alg<64, false>(a, alg);
   if (N == 32) return prune ? emu3_alg<32, true>(a, alg) : emu3_alg<32, false>(a, alg);
   return -2;

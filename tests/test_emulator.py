@@ -116,11 +116,11 @@ def test_emulated_masked_skip(emu):
 
 
 BIG = [((64, 64), (32, 32), (32, 32)), ((40, 48), (30, 24), (20, 24)), ((72, 40), (20, 30), (24, 20)),
-       ((64, 32), (32, 40), (32, 24))]
+       ((64, 32), (32, 40), (32, 24)), ((16, 24), (48, 40), (16, 16))]
 
 
 @pytest.mark.parametrize("alg", ["fft", "zncc", "nsqecc"])
-@pytest.mark.parametrize("cfg", BIG, ids=["is64", "aniso", "unpruned", "wide_sm"])
+@pytest.mark.parametrize("cfg", BIG, ids=["is64", "aniso", "unpruned", "wide_sm", "lags97"])
 def test_emulated_big_window_matches_oracle(emu, alg, cfg):
     """Search windows 65..128: the 128-thread block kernel's phases."""
     IS, SM, st = cfg

@@ -73,6 +73,18 @@ CASES = [
 ]
 
 
+@pytest.mark.parametrize("alg", ["fft", "nsqecc"])
+def test_emulated_3d_length128_matches_oracle(emu, alg):
+    """Search windows 65..128 (here 96): the 3D kernels at FFT length 128."""
+    shape, IS, SM, st = (104, 96, 96), (32, 32, 32), (32, 32, 32), (48, 48, 48)
+    i1, i2, _ = synth.pair_3d_shear(shape=shape, seed_stream=36, shift=(9.4, -7.3, 5.2))
+    po = O.set_piv_parameters(corr_alg=alg, interSize=IS, searchMargin=SM, step=st, computeSN=True)
+    po.ndims = 3
+    VFo, SNo, Co = O.piv_single_pass(i1, i2, po, keep_corr=True)
+    VF, SN, PL = run_emu3(emu, i1, i2, alg, IS, SM, st)
+    check_against(VF, SN, PL, VFo, SNo, Co, shape, IS, SM, st)
+
+
 @pytest.mark.parametrize("alg", ["fft", "zncc", "nsqecc"])
 @pytest.mark.parametrize("cfg", CASES, ids=["n32", "n64", "n32full", "aniso"])
 def test_emulated_3d_matches_oracle(emu, alg, cfg):

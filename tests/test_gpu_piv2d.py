@@ -115,7 +115,8 @@ def test_double_masked_skip(gpu):
 
 @pytest.mark.parametrize("alg", ["fft", "zncc", "nsqecc"])
 @pytest.mark.parametrize("cfg", [((64, 64), (32, 32), (32, 32)), ((40, 48), (30, 24), (20, 24)),
-                                 ((72, 40), (20, 30), (24, 20))], ids=["is64", "aniso", "unpruned"])
+                                 ((72, 40), (20, 30), (24, 20)), ((16, 24), (48, 40), (16, 16))],
+                         ids=["is64", "aniso", "unpruned", "lags97"])
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 def test_piv2d_big_window_matches_oracle(alg, cfg, dtype, gpu):
     """Search windows 65..128 run on the 128-thread block kernel."""

@@ -67,6 +67,20 @@ def test_piv3d_matches_oracle(alg, cfg, dtype, gpu):
     _check(VF, SN, planes, VFo, SNo, Co, shape, IS, SM, st)
 
 
+@pytest.mark.parametrize("alg", ["fft", "zncc", "nsqecc"])
+def test_piv3d_length128_matches_oracle(alg, gpu):
+    """Search windows 65..128 (here 96): the 3D kernels at FFT length 128."""
+    shape, IS, SM, st = (104, 96, 96), (32, 32, 32), (32, 32, 32), (48, 48, 48)
+    i1, i2, _ = synth.pair_3d_shear(shape=shape, seed_stream=36, shift=(9.4, -7.3, 5.2))
+    po = O.set_piv_parameters(corr_alg=alg, interSize=IS, searchMargin=SM, step=st, computeSN=True)
+    po.ndims = 3
+    VFo, SNo, Co = O.piv_single_pass(i1, i2, po, keep_corr=True)
+    pp = _params(alg, IS, SM, st)
+    VF, SN = PIV(i1, i2, pp)
+    planes = correlation_planes(i1, i2, pp)
+    _check(VF, SN, planes, VFo, SNo, Co, shape, IS, SM, st)
+
+
 def test_piv3d_masked(gpu):
     shape, IS, SM, st = (48, 44, 40), (16, 16, 16), (8, 8, 8), (8, 8, 8)
     i1, i2, _ = synth.pair_3d_shear(shape=shape, seed_stream=32, dtype=np.float64)
