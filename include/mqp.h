@@ -203,6 +203,51 @@ MQP_API int mqp_batch_plan_info(const mqp_plan* plan, int64_t* total_ia, int64_t
 MQP_API int mqp_batch_plan_destroy(mqp_plan* plan);
 
 /*
+ * Serving.  No counterpart in the reference (a serial per-call PIV): a
+ * request loop for time-lapse streams.  Each stream (fixed frame size, dtype
+ * and single-pass PIV parameters) keeps its last frames and their integral
+ * images resident on the device; every submitted frame t+1 becomes one
+ * request PIV(frame t, frame t+1), admitted continuously by a worker thread
+ * as execution slots and the device-memory budget free up, its work
+ * overlapping on the device with the other slots'.  Results are identical to
+ * mqp_piv on the same pair.  Frames are host arrays (copied at submit).
+ */
+typedef struct mqp_server mqp_server;
+
+typedef struct mqp_server_options {
+  int32_t slots;              /* concurrent requests on the device (default 4) */
+  int32_t reserved0;
+  int64_t hbm_budget_bytes;   /* transient device bytes requests may hold (0 = free memory - reserve) */
+  int64_t hbm_reserve_bytes;  /* kept free when the budget is derived (default 4 GiB) */
+  int64_t chunk3d_budget;     /* 3D chunk scratch per request (default 512 MiB) */
+  int32_t reserved[8];
+} mqp_server_options;
+
+typedef struct mqp_server_stats {
+  int64_t completed, failed, queued, running;
+  int64_t admitted_while_busy;  /* requests admitted while other slots were running */
+  double p50_ms, p99_ms, max_ms; /* submit -> result latency of completed requests */
+  int64_t ia_done;
+  double ia_per_s;              /* completed IAs / (last completion - first submit) */
+  int64_t budget_bytes, in_use_bytes;
+} mqp_server_stats;
+
+MQP_API int mqp_server_create(int device, const mqp_server_options* opt /* NULL = defaults */, mqp_server** out);
+/* A stream: its first frame (host, column-major) and the parameters of every request. */
+MQP_API int mqp_server_open_stream(mqp_server* srv, const void* first_frame, int dtype, int ndims, const int64_t dims[3],
+                                   const mqp_params* p, int32_t* stream_id);
+/* Queue PIV(previous frame, frame) of a stream; returns immediately. */
+MQP_API int mqp_server_submit(mqp_server* srv, int32_t stream_id, const void* frame, uint64_t* request_id);
+/* Collect a request's VF/SN (host, shapes as mqp_piv) and its latency: wait_ms = 0 polls
+ * (MQP_ERR_BUSY while running), < 0 waits, > 0 waits at most that long (MQP_ERR_TIMEOUT). */
+MQP_API int mqp_server_result(mqp_server* srv, uint64_t request_id, int32_t wait_ms, double* VF, double* SN,
+                              double* latency_ms);
+MQP_API int mqp_server_get_stats(mqp_server* srv, mqp_server_stats* out);
+MQP_API int mqp_server_reset_stats(mqp_server* srv);
+MQP_API const char* mqp_server_last_error(const mqp_server* srv);
+MQP_API int mqp_server_destroy(mqp_server* srv);
+
+/*
  * Vector-field post-processing: the local-window operations of
  * src/postprocessing/postprocessing.jl on a Float64 field of `ncomp`
  * components over an `ndims`-D grid (column-major, component fastest: the

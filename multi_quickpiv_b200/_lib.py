@@ -76,6 +76,18 @@ class MqpBatchOptions(C.Structure):
                 ("chunk3d_budget", C.c_int64), ("reserved", C.c_int32 * 8)]
 
 
+class MqpServerOptions(C.Structure):
+    _fields_ = [("slots", C.c_int32), ("reserved0", C.c_int32), ("hbm_budget_bytes", C.c_int64),
+                ("hbm_reserve_bytes", C.c_int64), ("chunk3d_budget", C.c_int64), ("reserved", C.c_int32 * 8)]
+
+
+class MqpServerStats(C.Structure):
+    _fields_ = [("completed", C.c_int64), ("failed", C.c_int64), ("queued", C.c_int64), ("running", C.c_int64),
+                ("admitted_while_busy", C.c_int64), ("p50_ms", C.c_double), ("p99_ms", C.c_double),
+                ("max_ms", C.c_double), ("ia_done", C.c_int64), ("ia_per_s", C.c_double),
+                ("budget_bytes", C.c_int64), ("in_use_bytes", C.c_int64)]
+
+
 class MqpField(C.Structure):
     _fields_ = [("ncomp", C.c_int32), ("ndims", C.c_int32), ("dims", C.c_int64 * 4)]
 
@@ -126,6 +138,16 @@ SIGNATURES = {
     "mqp_batch_plan_run": (C.c_int, [C.c_void_p, C.c_void_p]),
     "mqp_batch_plan_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "mqp_batch_plan_destroy": (C.c_int, [C.c_void_p]),
+    "mqp_server_create": (C.c_int, [C.c_int, C.POINTER(MqpServerOptions), C.POINTER(C.c_void_p)]),
+    "mqp_server_open_stream": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, I64x3, C.POINTER(MqpParams),
+                                         C.POINTER(C.c_int32)]),
+    "mqp_server_submit": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.POINTER(C.c_uint64)]),
+    "mqp_server_result": (C.c_int, [C.c_void_p, C.c_uint64, C.c_int32, C.c_void_p, C.c_void_p,
+                                    C.POINTER(C.c_double)]),
+    "mqp_server_get_stats": (C.c_int, [C.c_void_p, C.POINTER(MqpServerStats)]),
+    "mqp_server_reset_stats": (C.c_int, [C.c_void_p]),
+    "mqp_server_last_error": (C.c_char_p, [C.c_void_p]),
+    "mqp_server_destroy": (C.c_int, [C.c_void_p]),
     "mqp_postprocess_device": (C.c_int, [C.c_void_p, C.POINTER(MqpPostParams), C.POINTER(MqpField), C.c_void_p,
                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "mqp_postprocess": (C.c_int, [C.c_void_p, C.POINTER(MqpPostParams), C.POINTER(MqpField), C.c_void_p,

@@ -182,6 +182,7 @@ int run_pass_3d(mqp_ctx* ctx, const Problem& pb, const mqp_params* p, const void
       a.II1 = (const double*)ctx->II1.ptr;
     }
   }
+  const bool direct = mqp::direct3d_ok(pb.IS, pb.SM);  // small windows: spatial correlation, no chunk scratch
   // chunk scratch: Gz | Fz | C | C2 | V | state, each 256-byte aligned
   const size_t per_ia = mqp::piv3d_scratch_bytes_per_ia(pb.IS, pb.SM, pb.alg);
   const int64_t n = ia_end - ia_begin;
@@ -200,8 +201,9 @@ int run_pass_3d(mqp_ctx* ctx, const Problem& pb, const mqp_params* p, const void
   const size_t bC2 = pb.alg == mqp::ALG_MASK_NSQECC ? bC : 0;
   const size_t bV = align256(c * P12 * P3 * sizeof(float));
   const size_t bS = align256(c * sizeof(mqp::IA3State));
-  if ((e = ctx->scratch3d.ensure(bGz + bFz + bC + bC2 + bV + bS)) != cudaSuccess) return cuda_fail(ctx, e, "3D scratch");
-  char* base = (char*)ctx->scratch3d.ptr;
+  if (!direct && (e = ctx->scratch3d.ensure(bGz + bFz + bC + bC2 + bV + bS)) != cudaSuccess)
+    return cuda_fail(ctx, e, "3D scratch");
+  char* base = direct ? nullptr : (char*)ctx->scratch3d.ptr;
   a.Gz = (float2*)base;
   a.Fz = (float2*)(base + bGz);
   a.C = (float2*)(base + bGz + bFz);

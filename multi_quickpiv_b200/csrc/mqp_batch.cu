@@ -141,8 +141,10 @@ int mqp_batch_plan_create(mqp_ctx* ctx, const mqp_batch_item* items, int32_t n_i
         if (mqp::piv3d_fft_len(SS) == 0)
           return fail(ctx, MQP_ERR_UNSUPPORTED, who + "3D search window (interSize + 2 searchMargin) too large at pass scale " +
                                                     std::to_string(1 << l));
-        const size_t per = mqp::piv3d_scratch_bytes_per_ia(pb.IS, pb.SM, pb.alg);
-        scr3d_per = std::max(scr3d_per, per * (size_t)chunk_for(o, per, pb.n_ia));
+        if (!mqp::direct3d_ok(pb.IS, pb.SM)) {  // the direct kernel needs no chunk scratch
+          const size_t per = mqp::piv3d_scratch_bytes_per_ia(pb.IS, pb.SM, pb.alg);
+          scr3d_per = std::max(scr3d_per, per * (size_t)chunk_for(o, per, pb.n_ia));
+        }
       }
     }
     ip.alg = ip.lev[0].pb.alg;
@@ -191,8 +193,10 @@ int mqp_batch_plan_create(mqp_ctx* ctx, const mqp_batch_item* items, int32_t n_i
       if (l < 0 || ip.it.ndims != 2) continue;
       const Problem& pb = ip.lev[l].pb;
       if (pb.n_ia == 0) continue;
-      const int N = mqp::piv2d_fft_len(pb.IS[0] + 2 * pb.SM[0], pb.IS[1] + 2 * pb.SM[1]);
-      const bool prune = pb.IS[0] <= N / 2 && pb.IS[1] <= N / 2;
+      // kernel variant: N = 1 marks the direct (spatial) correlation of small windows
+      const bool direct = mqp::direct2d_ok(pb.IS[0], pb.IS[1], pb.SM[0], pb.SM[1]);
+      const int N = direct ? 1 : mqp::piv2d_fft_len(pb.IS[0] + 2 * pb.SM[0], pb.IS[1] + 2 * pb.SM[1]);
+      const bool prune = direct || (pb.IS[0] <= N / 2 && pb.IS[1] <= N / 2);
       const auto key = std::make_tuple(N, (int)prune, ip.alg, (int)ip.it.dtype);
       auto f = idx.find(key);
       if (f == idx.end()) {
@@ -207,8 +211,9 @@ int mqp_batch_plan_create(mqp_ctx* ctx, const mqp_batch_item* items, int32_t n_i
       }
       Group& g = groups[r][f->second];
       g.members.push_back(k);
-      g.wf2 = std::max(g.wf2, mqp::piv2d_warp_f2(N, prune, 2 * pb.SM[0] + 1, 2 * pb.SM[1] + 1,
-                                                 ip.alg == mqp::ALG_MASK_NSQECC));
+      g.wf2 = std::max(g.wf2, direct ? (mqp::piv2d_direct_words(pb.IS[0], pb.IS[1], pb.SM[0], pb.SM[1]) + 1) / 2
+                                     : mqp::piv2d_warp_f2(N, prune, 2 * pb.SM[0] + 1, 2 * pb.SM[1] + 1,
+                                                          ip.alg == mqp::ALG_MASK_NSQECC));
     }
     for (Group& g : groups[r]) {
       g.items_off = ar.take(g.members.size() * sizeof(mqp::Piv2dArgs));
@@ -425,7 +430,7 @@ int mqp_batch_plan_create(mqp_ctx* ctx, const mqp_batch_item* items, int32_t n_i
       a.mask_threshold = ip.it.params.mask_threshold;
       const int alg = pb.alg;
       const int64_t chunks = (pb.n_ia + chunk - 1) / chunk;
-      P->launches += chunks * (alg == mqp::ALG_MASK_NSQECC ? 5 : 3);
+      P->launches += mqp::direct3d_ok(pb.IS, pb.SM) ? 1 : chunks * (alg == mqp::ALG_MASK_NSQECC ? 5 : 3);
       P->total_ia += pb.n_ia;
       P->ops.push_back([=](cudaStream_t, cudaStream_t s) {
         std::string err;

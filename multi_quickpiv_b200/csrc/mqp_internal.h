@@ -10,6 +10,7 @@
 #include "mqp_piv3d.cuh"
 #include "mqp_multipass.cuh"
 #include "mqp_post.cuh"
+#include "mqp_direct.cuh"
 
 namespace mqp {
 
@@ -58,6 +59,14 @@ struct Piv2dBatch {
 };
 int piv2d_warp_f2(int N, bool prune, int P1, int P2, bool masked);
 cudaError_t launch_piv2d_batch(const Piv2dBatch& b, cudaStream_t s, std::string& err);
+
+// Small windows (direct2d_ok / direct3d_ok): spatial correlation, one warp
+// per IA (mqp_direct.cu).  Batch plans mark these groups with N = 1; their
+// Piv2dBatch::wf2 is half the per-warp word count (piv2d_direct_words).
+int piv2d_direct_words(int IS1, int IS2, int SM1, int SM2);
+cudaError_t launch_piv2d_direct(const Piv2dArgs& a, int alg, cudaStream_t s, std::string& err);
+cudaError_t launch_piv2d_direct_batch(const Piv2dBatch& b, cudaStream_t s, std::string& err);
+cudaError_t launch_piv3d_direct(const Piv3dArgs& a, int alg, cudaStream_t s, std::string& err);
 
 // Search windows 65..128 (FFT length 128): one 128-thread block per IA
 // (mqp_piv2d_big.cu); for these, Piv2dBatch::wf2 is the block's whole

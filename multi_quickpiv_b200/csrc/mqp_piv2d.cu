@@ -584,6 +584,7 @@ static cudaError_t launch_batch_dt(const Piv2dBatch& b, cudaStream_t s, std::str
 cudaError_t launch_piv2d_batch(const Piv2dBatch& b, cudaStream_t s, std::string& err) {
   if (b.total <= 0 || b.n_items <= 0) return cudaSuccess;
   if (b.N == 128) return launch_piv2d_big_batch(b, s, err);
+  if (b.N == 1) return launch_piv2d_direct_batch(b, s, err);
   if (b.N == 64) return b.prune ? launch_batch_dt<64, true>(b, s, err) : launch_batch_dt<64, false>(b, s, err);
   if (b.N == 32) return b.prune ? launch_batch_dt<32, true>(b, s, err) : launch_batch_dt<32, false>(b, s, err);
   err = "search window larger than 64 along some axis is not supported by the 2D kernel";
@@ -591,6 +592,7 @@ cudaError_t launch_piv2d_batch(const Piv2dBatch& b, cudaStream_t s, std::string&
 }
 
 cudaError_t launch_piv2d(const Piv2dArgs& a, int alg, cudaStream_t s, std::string& err) {
+  if (direct2d_ok(a.IS1, a.IS2, a.SM1, a.SM2)) return launch_piv2d_direct(a, alg, s, err);
   const int SS1 = a.IS1 + 2 * a.SM1, SS2 = a.IS2 + 2 * a.SM2;
   const int N = piv2d_fft_len(SS1, SS2);
   const bool prune = (a.IS1 <= N / 2) && (a.IS2 <= N / 2);

@@ -233,11 +233,12 @@ size_t piv3d_scratch_bytes_per_ia(const int IS[3], const int SM[3], int alg) {
 cudaError_t launch_piv3d(const Piv3dArgs& a, int alg, long long chunk, cudaStream_t s, std::string& err) {
   const int SS[3] = {a.IS[0] + 2 * a.SM[0], a.IS[1] + 2 * a.SM[1], a.IS[2] + 2 * a.SM[2]};
   const int N = piv3d_fft_len(SS);
-  if (chunk < 1 || chunk > 65535) {
+  if (!direct3d_ok(a.IS, a.SM) && (chunk < 1 || chunk > 65535)) {
     err = "3D chunk must be in [1, 65535]";
     return cudaErrorInvalidValue;
   }
   if (a.ia_end <= a.ia_begin) return cudaSuccess;
+  if (direct3d_ok(a.IS, a.SM)) return launch_piv3d_direct(a, alg, s, err);  // small windows: no chunk scratch
   const bool prune = piv3d_prune(a.IS, N);
   if (N == 64) return prune ? run_dt<64, true>(a, alg, chunk, s, err) : run_dt<64, false>(a, alg, chunk, s, err);
   if (N == 32) return prune ? run_dt<32, true>(a, alg, chunk, s, err) : run_dt<32, false>(a, alg, chunk, s, err);

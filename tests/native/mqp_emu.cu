@@ -9,6 +9,7 @@
 
 #include <vector>
 
+#include "mqp_direct.cuh"
 #include "mqp_piv2d.cuh"
 
 using namespace mqp;
@@ -168,7 +169,8 @@ static int emu_alg(const Piv2dArgs& a, int alg) {
   return 0;
 }
 
-int emu_piv2d_big(const Piv2dArgs& a, int alg);  // mqp_emu_big.cu
+int emu_piv2d_big(const Piv2dArgs& a, int alg);     // mqp_emu_big.cu
+int emu_piv2d_direct(const Piv2dArgs& a, int alg);  // mqp_emu_direct.cu
 
 extern "C" __attribute__((visibility("default"))) int mqp_emu_piv2d(
     const void* img1, const void* img2, const void* mask, const void* mask_skip, int dtype, int H, int W,
@@ -206,6 +208,7 @@ extern "C" __attribute__((visibility("default"))) int mqp_emu_piv2d(
   const int SS = (IS1 + 2 * SM1) > (IS2 + 2 * SM2) ? (IS1 + 2 * SM1) : (IS2 + 2 * SM2);
   const int N = SS <= 32 ? 32 : (SS <= 64 ? 64 : (SS <= 128 ? 128 : 0));
   const bool prune = IS1 <= N / 2 && IS2 <= N / 2;
+  if (direct2d_ok(IS1, IS2, SM1, SM2)) return emu_piv2d_direct(a, alg);
   if (N == 128) return emu_piv2d_big(a, alg);
   if (N == 64) return prune ? emu_alg<64, true>(a, alg) : emu_alg<64, false>(a, alg);
   if (N == 32) return prune ? emu_alg<32, true>(a, alg) : emu_alg<32, false>(a, alg);

@@ -10,9 +10,12 @@
 #include <vector>
 
 #include "mqp_multipass.cuh"
+#include "mqp_direct.cuh"
 #include "mqp_piv3d.cuh"
 
 using namespace mqp;
+
+int emu_piv3d_direct(const Piv3dArgs& a, int alg);  // mqp_emu_direct.cu
 
 // exclusive-prefix integral volume (H+1) x (W+1) x (D+1)
 static void integral3(const void* img, int dtype, int H, int W, int D, bool sq, std::vector<double>& out) {
@@ -172,6 +175,7 @@ extern "C" __attribute__((visibility("default"))) int mqp_emu_piv3d(
   a.ia_end = ia_end;
   a.threshold = threshold;
   a.mask_threshold = mask_threshold;
+  if (direct3d_ok(a.IS, a.SM)) return emu_piv3d_direct(a, alg);
   const int N = SS <= 32 ? 32 : (SS <= 64 ? 64 : (SS <= 128 ? 128 : 0));
   const bool prune = IS[0] <= N / 2 && IS[1] <= N / 2 && IS[2] <= N / 2;
   if (N == 128) return prune ? emu3_alg<128, true>(a, alg) : -2;

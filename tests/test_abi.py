@@ -30,7 +30,9 @@ def test_library_exports_every_declared_symbol():
 
 @pytest.mark.parametrize("cname,py", [("mqp_params", "MqpParams"), ("mqp_profile", "MqpProfile"),
                                       ("mqp_field", "MqpField"), ("mqp_post_params", "MqpPostParams"),
-                                      ("mqp_batch_item", "MqpBatchItem"), ("mqp_batch_options", "MqpBatchOptions")])
+                                      ("mqp_batch_item", "MqpBatchItem"), ("mqp_batch_options", "MqpBatchOptions"),
+                                      ("mqp_server_options", "MqpServerOptions"),
+                                      ("mqp_server_stats", "MqpServerStats")])
 def test_abi_version_and_struct_layout(tmp_path, cname, py):
     """Each ctypes mirror matches the C layout (size and every field offset),
     checked by compiling a probe against include/mqp.h."""

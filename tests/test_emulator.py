@@ -150,3 +150,40 @@ def test_emulated_big_window_masked(emu):
     assert worst <= MASK_PLANE_RTOL, worst
     bad = (np.abs(VF - VFo) > VF_ATOL).any(axis=0) & ~near_tie
     assert not bad.any(), np.abs(VF - VFo).max()
+
+
+SMALL = [((8, 8), (4, 4), (8, 8)), ((4, 4), (2, 2), (4, 4)), ((6, 8), (3, 2), (5, 6)), ((12, 8), (2, 3), (6, 8))]
+
+
+@pytest.mark.parametrize("alg", ["fft", "zncc", "nsqecc"])
+@pytest.mark.parametrize("cfg", SMALL, ids=["is8", "is4", "aniso", "is12x8"])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_emulated_direct_small_windows(emu, alg, cfg, dtype):
+    """Small windows take the direct (spatial) correlation kernel."""
+    IS, SM, st = cfg
+    i1, i2, _ = synth.pair_2d_shift(shape=(72, 68), shift=(1.3, -0.6), seed_stream=26)
+    i1, i2 = i1.astype(dtype), i2.astype(dtype)
+    po = O.set_piv_parameters(corr_alg=alg, interSize=IS, searchMargin=SM, step=st, computeSN=True)
+    po.ndims = 2
+    VFo, SNo, Co = O.piv_single_pass(i1, i2, po, keep_corr=True)
+    VF, SN, PL = run_emu(emu, i1, i2, alg, IS, SM, st)
+    worst, near_tie = compare_planes(PL, Co, i1.shape, IS, SM, st)
+    assert worst <= PLANE_RTOL, worst
+    bad = (np.abs(VF - VFo) > VF_ATOL).any(axis=0) & ~near_tie
+    assert not bad.any(), np.abs(VF - VFo).max()
+    assert (sn_ok(SN, SNo) | near_tie | ~np.isfinite(SNo)).all()
+
+
+def test_emulated_direct_masked(emu):
+    IS, SM, st = (8, 8), (4, 4), (8, 8)
+    i1, i2, _ = synth.pair_2d_shift(shape=(72, 72), shift=(1.2, 2.1), seed_stream=27)
+    mask = synth.ellipse_mask(np.random.default_rng(4), i1.shape, cover=0.7)
+    po = O.set_piv_parameters(interSize=IS, searchMargin=SM, step=st, computeSN=True)
+    po.ndims = 2
+    VFo, SNo, Co = O.piv_single_pass(i1, i2, po, mask=mask, keep_corr=True)
+    VF, SN, PL = run_emu(emu, i1, i2, "nsqecc", IS, SM, st, mask=mask)
+    sparse = mask_coverage(mask, i1.shape, IS, st) < 0.25
+    worst, near_tie = compare_planes(PL, Co, i1.shape, IS, SM, st, skip=sparse)
+    assert worst <= MASK_PLANE_RTOL, worst
+    bad = (np.abs(VF - VFo) > VF_ATOL).any(axis=0) & ~near_tie & ~sparse
+    assert not bad.any(), np.abs(VF - VFo).max()

@@ -125,3 +125,38 @@ def test_emulated_3d_threshold_skip(emu):
     VF, SN, _ = run_emu3(emu, i1, i2, "fft", IS, SM, st, thr=0.0)
     assert np.all(VF[:, 0, 0, 0] == 0) and SN[0, 0, 0] == 0 and np.all(VFo[:, 0, 0, 0] == 0)
     assert np.max(np.abs(VF - VFo)) < VF_ATOL
+
+
+@pytest.mark.parametrize("alg", ["fft", "zncc", "nsqecc"])
+@pytest.mark.parametrize("cfg", [((24, 20, 20), (4, 4, 4), (2, 2, 2), (4, 4, 4)),
+                                 ((28, 24, 24), (8, 8, 8), (4, 4, 4), (8, 8, 8)),
+                                 ((24, 24, 20), (6, 4, 8), (2, 3, 2), (6, 5, 6))], ids=["is4", "is8", "aniso"])
+def test_emulated_3d_direct_small_windows(emu, alg, cfg):
+    """Small 3D windows take the direct (spatial) correlation kernel."""
+    shape, IS, SM, st = cfg
+    i1, i2, _ = synth.pair_3d_shear(shape=shape, seed_stream=37, shift=(1.3, -0.7, 0.9), shear=0.0)
+    po = O.set_piv_parameters(corr_alg=alg, interSize=IS, searchMargin=SM, step=st, computeSN=True)
+    po.ndims = 3
+    VFo, SNo, Co = O.piv_single_pass(i1, i2, po, keep_corr=True)
+    VF, SN, PL = run_emu3(emu, i1, i2, alg, IS, SM, st)
+    worst, near_tie = compare_planes(PL, Co, shape, IS, SM, st)
+    assert worst <= PLANE_RTOL, worst
+    bad = (np.abs(VF - VFo) > VF_ATOL).any(axis=0) & ~near_tie
+    assert not bad.any(), np.abs(VF - VFo).max()
+    assert (sn_ok(SN, SNo) | near_tie | ~np.isfinite(SNo)).all()
+
+
+def test_emulated_3d_direct_masked(emu):
+    shape, IS, SM, st = (24, 24, 24), (8, 8, 8), (4, 4, 4), (4, 4, 4)
+    i1, i2, _ = synth.pair_3d_shear(shape=shape, seed_stream=38, shift=(1.2, 0.4, -0.8), shear=0.0,
+                                    dtype=np.float64)
+    mask = synth.ellipse_mask(np.random.default_rng(6), shape, cover=0.7)
+    po = O.set_piv_parameters(interSize=IS, searchMargin=SM, step=st, computeSN=True)
+    po.ndims = 3
+    VFo, SNo, Co = O.piv_single_pass(i1, i2, po, mask=mask, keep_corr=True)
+    VF, SN, PL = run_emu3(emu, i1, i2, "nsqecc", IS, SM, st, mask=mask)
+    sparse = mask_coverage(mask, shape, IS, st) < 0.25
+    worst, near_tie = compare_planes(PL, Co, shape, IS, SM, st, skip=sparse)
+    assert worst <= MASK_PLANE_RTOL, worst
+    bad = (np.abs(VF - VFo) > VF_ATOL).any(axis=0) & ~near_tie & ~sparse
+    assert not bad.any(), np.abs(VF - VFo).max()
