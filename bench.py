@@ -342,6 +342,218 @@ def run_ours(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# the batched workload: 64 mixed pairs, 3-pass refinement (windows halving)
+# ---------------------------------------------------------------------------
+def batch_pairs(size_scale=1.0):
+    """64 pairs of mixed size and dimensionality; interSize drawn from
+    {16, 32, 64} is the coarsest pass's window, halved on each of 3 passes
+    (the final pass uses interSize/4, searchMargin interSize/8, step = window)."""
+    import multi_quickpiv_b200 as mq
+    from multi_quickpiv_b200 import synth
+    pairs = []
+    for it in synth.batch_mixed(64, size_scale=size_scale):
+        nd = it.img1.ndim
+        IS = it.interSize // 4
+        p = mq.setPIVParameters(corr_alg=it.corr_alg, interSize=(IS,) * nd, searchMargin=(max(IS // 2, 1),) * nd,
+                                step=(IS,) * nd, multipass=3, refine=True, computeSN=False)
+        pairs.append((it.img1, it.img2, p) + ((it.mask,) if it.mask is not None else ()))
+    return pairs
+
+
+def pass_flops(pairs):
+    """Reference-equivalent FLOPs of every pass of every pair (FFT of the
+    search-window size per axis, the reference's unpruned convention)."""
+    total, n_ia = 0.0, 0
+    for pr in pairs:
+        shape, p = pr[0].shape, pr[2]
+        nd = len(shape)
+        for lvl in range(p.multipass):
+            sc = 2 ** lvl
+            IS, SM = p.interSize[0] * sc, p.searchMargin[0] * sc
+            st = p.step[0] * sc
+            vf = [(n - IS) // st + 1 if n >= IS else 0 for n in shape]
+            n = int(np.prod(vf))
+            total += n * flops_per_ia(cs=IS + 2 * SM, P=2 * SM + 1, IS=IS, norm=p.corr_alg != "fftcc", nd=nd)
+            n_ia += n
+    return total, n_ia
+
+
+def run_batch(args):
+    import torch
+
+    import multi_quickpiv_b200 as mq
+    from multi_quickpiv_b200 import tune
+    t0 = time.time()
+    pairs = batch_pairs()
+    gen_s = time.time() - t0
+    dev = torch.device("cuda", 0)
+    s = torch.cuda.current_stream(dev)
+    # plain fused path: one PIV call per pair on device-resident images
+    dp = []
+    for pr in pairs:
+        t1 = mq.piv._colmajor_torch(torch.from_numpy(pr[0]).to(dev))
+        t2 = mq.piv._colmajor_torch(torch.from_numpy(pr[1]).to(dev))
+        tm = mq.piv._colmajor_torch(torch.from_numpy(np.asarray(pr[3], np.float32)).to(dev)) if len(pr) > 3 else None
+        dp.append((t1, t2, pr[2], tm))
+
+    def plain():
+        for t1, t2, p, tm in dp:
+            mq.PIV(t1, t2, *([tm] if tm is not None else []), p)
+    for _ in range(max(1, args.warmup // 2)):
+        plain()
+    ms_plain = tune.time_ms(plain, s, max(1, args.steps // 4))
+    best, tuning, plan = tune.autotune_batch(pairs)
+    for _ in range(args.warmup):
+        plan.run()
+    torch.cuda.synchronize()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(0) as clk:
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            ev[k][0].record(s)
+            plan.run()
+            ev[k][1].record(s)
+        torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in ev) / args.steps
+    info = plan.info()
+    flops, n_ia = pass_flops(pairs)
+    # e2e: every pair's images copied in from pinned host memory, the plan run,
+    # every VF read back
+    hosts = []
+    for k, pr in enumerate(pairs):
+        t1, t2 = plan._keep[6 * k], plan._keep[6 * k + 1]
+        h1 = torch.empty_like(t1, device="cpu").pin_memory()
+        h2 = torch.empty_like(t2, device="cpu").pin_memory()
+        h1.copy_(t1)
+        h2.copy_(t2)
+        hosts.append((h1, h2, t1, t2))
+    h2d = sum(h1.numel() * h1.element_size() * 2 for h1, _, _, _ in hosts)
+    d2h = sum(VF.numel() * 8 for VF, _ in plan.results())
+    e2e = []
+    for k in range(max(2, args.steps // 4)):
+        torch.cuda.synchronize()
+        ta = time.perf_counter()
+        for h1, h2, t1, t2 in hosts:
+            t1.copy_(h1, non_blocking=True)
+            t2.copy_(h2, non_blocking=True)
+        plan.run()
+        outs = [VF.cpu() for VF, _ in plan.results()]
+        e2e.append(time.perf_counter() - ta)
+    peaks, src = measured_peaks()
+    fp32_peak = 148 * 128 * 2 * peaks.get("sm_max_mhz", 1965.0) * 1e6
+    value = info["total_ia"] / (ms / 1e3)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "batch of 64 mixed pairs (2D 512^2-4096x2048, 3D 128^3-256^3), 3-pass refinement, "
+                                   "interSize {16,32,64} halving, 25% masked NSQECC",
+                       "pairs": len(pairs), "ia_all_passes": info["total_ia"], "generation_s": gen_s,
+                       "plan": best, "tuning_ms": tuning, "plan_scratch_bytes": info["scratch_bytes"],
+                       "l2": "flushed between steps by a 256 MiB write outside the timed events"},
+            "plain_path": {"ms_per_step": ms_plain, "value": info["total_ia"] / (ms_plain / 1e3),
+                           "what": "one PIV call per pair on device-resident images, same kernels"},
+            "speedup_vs_plain": ms_plain / ms,
+            "e2e": {"value": info["total_ia"] * len(e2e) / sum(e2e), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": info["launches"] * args.steps,
+            "roofline": {"bound": "fp32", "achieved": flops / (ms / 1e3) / 1e12, "peak": fp32_peak / 1e12,
+                         "unit": "TFLOP/s", "frac": flops / (ms / 1e3) / fp32_peak, "traffic": None,
+                         "algorithmic_flop_per_step": flops,
+                         "peak_source": f"148 SM x 128 FP32 lanes x 2 x sm_max_mhz ({src})"},
+            "cpu_baseline": None, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    plan.close()
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# the serving workload: Poisson arrivals of 2D+t and 3D+t requests
+# ---------------------------------------------------------------------------
+def run_serve(args):
+    from multi_quickpiv_b200 import setPIVParameters, synth
+    from multi_quickpiv_b200.serve import Server
+    t0 = time.time()
+    kinds = []
+    # 2D+t: 2048^2 Float32, NSQECC IS 32 SM 16 step 8, 100 requests/s over 4 streams
+    for k in range(4):
+        tg = synth.TaylorGreenStream((2048, 2048), seed_stream=70 + k)
+        kinds.append(("2d", [tg.next() for _ in range(6)],
+                      setPIVParameters(corr_alg="nsqecc", interSize=32, searchMargin=16, step=8), 25.0))
+    # 3D+t: 256^3 Float32, FFTCC IS 32 SM 16 step 16, 5 requests/s
+    tg = synth.TaylorGreenStream((256, 256, 256), seed_stream=80)
+    kinds.append(("3d", [tg.next() for _ in range(4)],
+                  setPIVParameters(corr_alg="fft", interSize=32, searchMargin=16, step=16), 5.0))
+    gen_s = time.time() - t0
+    g = np.random.default_rng(2026)
+    horizon = args.steps / 105.0  # seconds of arrivals for ~steps requests
+    events = []
+    for ki, (_, frames, _, rate) in enumerate(kinds):
+        t = 0.0
+        while True:
+            t += g.exponential(1.0 / rate)
+            if t > horizon:
+                break
+            events.append((t, ki))
+    events.sort()
+    srv = Server(slots=4)
+    sids = [srv.open_stream(fr[0], p) for _, fr, p, _ in kinds]
+    for ki, (_, fr, _, _) in enumerate(kinds):  # warm-up: one request per stream
+        srv.result(srv.submit(sids[ki], fr[1]))
+    srv.reset_stats()
+    nxt = [2] * len(kinds)
+    rids = []
+    with ClockSampler(0) as clk:
+        ts = time.perf_counter()
+        for ta, ki in events:
+            while time.perf_counter() - ts < ta:
+                pass
+            fr = kinds[ki][1]
+            rids.append((ki, srv.submit(sids[ki], fr[nxt[ki] % len(fr)])))
+            nxt[ki] += 1
+        lat = {"2d": [], "3d": []}
+        for ki, rid in rids:
+            lat[kinds[ki][0]].append(srv.result(rid)[2])
+    st = srv.stats()
+    srv.close()
+    # plain per-request path: PIV() from host arrays, one request at a time, same arrivals
+    import multi_quickpiv_b200 as mq
+    plain = {"2d": [], "3d": []}
+    ts = time.perf_counter()
+    busy_until = 0.0
+    for ta, ki in events:
+        now = time.perf_counter() - ts
+        if now < ta:
+            time.sleep(ta - now)
+        fr, p = kinds[ki][1], kinds[ki][2]
+        mq.PIV(fr[0], fr[1], p)
+        plain[kinds[ki][0]].append((time.perf_counter() - ts - ta) * 1e3)
+
+    def pct(v, q):
+        return float(np.percentile(v, q)) if len(v) else None
+    ia2 = ((2048 - 32) // 8 + 1) ** 2
+    ia3 = ((256 - 32) // 16 + 1) ** 3
+    line = {"metric": METRIC, "value": st["ia_per_s"], "unit": UNIT, "n_gpus": 1, "steps": len(events),
+            "warmup": len(kinds), "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (Taylor-Green advected particle streams)",
+            "config": {"workload": "serving: Poisson arrivals, 2D+t 2048^2 NSQECC at 100/s (4 streams) and "
+                                   "3D+t 256^3 FFTCC at 5/s", "slots": 4, "frames_generation_s": gen_s,
+                       "ia_per_request": {"2d": ia2, "3d": ia3}},
+            "latency_ms": {"p50": st["p50_ms"], "p99": st["p99_ms"], "max": st["max_ms"],
+                           "2d_p50": pct(lat["2d"], 50), "2d_p99": pct(lat["2d"], 99),
+                           "3d_p50": pct(lat["3d"], 50), "3d_p99": pct(lat["3d"], 99)},
+            "admitted_while_busy": st["admitted_while_busy"], "completed": st["completed"], "failed": st["failed"],
+            "plain_path_latency_ms": {"2d_p50": pct(plain["2d"], 50), "2d_p99": pct(plain["2d"], 99),
+                                      "3d_p50": pct(plain["3d"], 50), "3d_p99": pct(plain["3d"], 99),
+                                      "what": "PIV() per request from host arrays, one at a time, same arrivals"},
+            "e2e": {"value": st["ia_per_s"], "unit": UNIT,
+                    "h2d_bytes_per_step": int(2048 * 2048 * 4), "d2h_bytes_per_step": int(ia2 * 2 * 8)},
+            "gpu_launches": None, "roofline": None, "cpu_baseline": None, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -352,12 +564,18 @@ def main(argv=None):
     ap.add_argument("--size", type=int, default=2048)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ref-budget", type=float, default=10.0)
-    ap.add_argument("--workload", default="vortex2048", choices=["vortex2048", "shear3d"],
-                    help="vortex2048: 2D vortex pair (--size, --alg); shear3d: 512x512x256 FFTCC volumes")
+    ap.add_argument("--workload", default="vortex2048", choices=["vortex2048", "shear3d", "batch64", "serve"],
+                    help="vortex2048: 2D vortex pair (--size, --alg); shear3d: 512x512x256 FFTCC volumes; "
+                         "batch64: 64 mixed pairs with 3-pass refinement (batch plans vs per-pair calls); "
+                         "serve: Poisson request streams (latency p50/p99; --steps = requests)")
     ap.add_argument("--chunk3d", type=int, default=0, help="IAs per 3D chunk (0: autotuned in warm-up)")
     args = ap.parse_args(argv)
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batch64":
+        return run_batch(args)
+    if args.workload == "serve":
+        return run_serve(args)
     return run_ours(args)
 
 
