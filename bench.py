@@ -190,8 +190,8 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 def kernel_launches(wl, chunk3d):
     """Kernels of this library one PIV call launches (counted from the code
-    path: integral scans, the fused 2D kernel or the three 3D kernels per
-    chunk)."""
+    path: integral scans, the fused 2D kernel, or per 3D chunk K3a, its
+    merge, K3b, K3c and its merge)."""
     scans = 0
     if wl.alg != "fft":
         per_image = 3 if wl.nd == 2 else 4  # cols, row chunks, row offsets (+ z scan)
@@ -199,7 +199,7 @@ def kernel_launches(wl, chunk3d):
     if wl.nd == 2:
         return scans + 1
     chunks = -(-wl.n_ia // chunk3d)
-    return scans + 3 * chunks
+    return scans + 5 * chunks
 
 
 def run_ours(args):
@@ -441,6 +441,14 @@ def run_batch(args):
         plan.run()
         outs = [VF.cpu() for VF, _ in plan.results()]
         e2e.append(time.perf_counter() - ta)
+    # the same pairs the way a caller of PIV() would run them without plans:
+    # one call per pair from host arrays (copies in, VF/SN out)
+    plain_e2e = []
+    for k in range(2):
+        ta = time.perf_counter()
+        for pr in pairs:
+            mq.PIV(pr[0], pr[1], *([pr[3]] if len(pr) > 3 else []), pr[2])
+        plain_e2e.append(time.perf_counter() - ta)
     peaks, src = measured_peaks()
     fp32_peak = 148 * 128 * 2 * peaks.get("sm_max_mhz", 1965.0) * 1e6
     value = info["total_ia"] / (ms / 1e3)
@@ -453,7 +461,9 @@ def run_batch(args):
                        "plan": best, "tuning_ms": tuning, "plan_scratch_bytes": info["scratch_bytes"],
                        "l2": "flushed between steps by a 256 MiB write outside the timed events"},
             "plain_path": {"ms_per_step": ms_plain, "value": info["total_ia"] / (ms_plain / 1e3),
-                           "what": "one PIV call per pair on device-resident images, same kernels"},
+                           "what": "one PIV call per pair on device-resident images, same kernels",
+                           "e2e_value": info["total_ia"] / min(plain_e2e),
+                           "e2e_what": "one PIV call per pair from host numpy arrays (best of 2 runs)"},
             "speedup_vs_plain": ms_plain / ms,
             "e2e": {"value": info["total_ia"] * len(e2e) / sum(e2e), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
@@ -542,7 +552,9 @@ def run_serve(args):
                        "ia_per_request": {"2d": ia2, "3d": ia3}},
             "latency_ms": {"p50": st["p50_ms"], "p99": st["p99_ms"], "max": st["max_ms"],
                            "2d_p50": pct(lat["2d"], 50), "2d_p99": pct(lat["2d"], 99),
-                           "3d_p50": pct(lat["3d"], 50), "3d_p99": pct(lat["3d"], 99)},
+                           "3d_p50": pct(lat["3d"], 50), "3d_p99": pct(lat["3d"], 99),
+                           "queued_p50": st["wait_p50_ms"], "queued_p99": st["wait_p99_ms"],
+                           "running_p50": st["run_p50_ms"], "running_p99": st["run_p99_ms"]},
             "admitted_while_busy": st["admitted_while_busy"], "completed": st["completed"], "failed": st["failed"],
             "plain_path_latency_ms": {"2d_p50": pct(plain["2d"], 50), "2d_p99": pct(plain["2d"], 99),
                                       "3d_p50": pct(plain["3d"], 50), "3d_p99": pct(plain["3d"], 99),

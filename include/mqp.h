@@ -230,6 +230,8 @@ typedef struct mqp_server_stats {
   int64_t ia_done;
   double ia_per_s;              /* completed IAs / (last completion - first submit) */
   int64_t budget_bytes, in_use_bytes;
+  double wait_p50_ms, wait_p99_ms; /* submit -> issue to a slot (queued) */
+  double run_p50_ms, run_p99_ms;   /* issue -> finished (on the device) */
 } mqp_server_stats;
 
 MQP_API int mqp_server_create(int device, const mqp_server_options* opt /* NULL = defaults */, mqp_server** out);

@@ -85,7 +85,8 @@ class MqpServerStats(C.Structure):
     _fields_ = [("completed", C.c_int64), ("failed", C.c_int64), ("queued", C.c_int64), ("running", C.c_int64),
                 ("admitted_while_busy", C.c_int64), ("p50_ms", C.c_double), ("p99_ms", C.c_double),
                 ("max_ms", C.c_double), ("ia_done", C.c_int64), ("ia_per_s", C.c_double),
-                ("budget_bytes", C.c_int64), ("in_use_bytes", C.c_int64)]
+                ("budget_bytes", C.c_int64), ("in_use_bytes", C.c_int64), ("wait_p50_ms", C.c_double),
+                ("wait_p99_ms", C.c_double), ("run_p50_ms", C.c_double), ("run_p99_ms", C.c_double)]
 
 
 class MqpField(C.Structure):

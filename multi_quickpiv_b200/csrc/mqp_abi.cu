@@ -183,33 +183,22 @@ int run_pass_3d(mqp_ctx* ctx, const Problem& pb, const mqp_params* p, const void
     }
   }
   const bool direct = mqp::direct3d_ok(pb.IS, pb.SM);  // small windows: spatial correlation, no chunk scratch
-  // chunk scratch: Gz | Fz | C | C2 | V | state, each 256-byte aligned
+  // chunk scratch: Gz | Fz | C | C2 | V | state | K3a parts | K3c parts
   const size_t per_ia = mqp::piv3d_scratch_bytes_per_ia(pb.IS, pb.SM, pb.alg);
   const int64_t n = ia_end - ia_begin;
   int64_t chunk = ctx->chunk3d > 0 ? ctx->chunk3d : (int64_t)(ctx->chunk3d_budget / per_ia);
   if (chunk < 1) chunk = 1;
   if (chunk > 65535) chunk = 65535;
   if (chunk > n) chunk = n;
-  const int N = mqp::piv3d_fft_len(SS);
-  const bool prune = pb.IS[0] <= N / 2 && pb.IS[1] <= N / 2 && pb.IS[2] <= N / 2;
-  const size_t K3 = N / 2 + 1, NF = prune ? N / 2 : N;
-  const size_t P12 = (size_t)(2 * pb.SM[0] + 1) * (2 * pb.SM[1] + 1), P3 = 2 * pb.SM[2] + 1;
-  const size_t c = (size_t)chunk;
-  const size_t bGz = align256(c * K3 * N * N * sizeof(float2));
-  const size_t bFz = align256(c * K3 * NF * NF * sizeof(float2));
-  const size_t bC = align256(c * K3 * P12 * sizeof(float2));
-  const size_t bC2 = pb.alg == mqp::ALG_MASK_NSQECC ? bC : 0;
-  const size_t bV = align256(c * P12 * P3 * sizeof(float));
-  const size_t bS = align256(c * sizeof(mqp::IA3State));
-  if (!direct && (e = ctx->scratch3d.ensure(bGz + bFz + bC + bC2 + bV + bS)) != cudaSuccess)
-    return cuda_fail(ctx, e, "3D scratch");
-  char* base = direct ? nullptr : (char*)ctx->scratch3d.ptr;
-  a.Gz = (float2*)base;
-  a.Fz = (float2*)(base + bGz);
-  a.C = (float2*)(base + bGz + bFz);
-  a.C2 = bC2 ? (float2*)(base + bGz + bFz + bC) : nullptr;
-  a.V = (float*)(base + bGz + bFz + bC + bC2);
-  a.state = (mqp::IA3State*)(base + bGz + bFz + bC + bC2 + bV);
+  for (int d = 0; d < 3; ++d) {
+    a.IS[d] = pb.IS[d];
+    a.SM[d] = pb.SM[d];
+  }
+  if (!direct) {
+    if ((e = ctx->scratch3d.ensure(mqp::piv3d_scratch_bytes(pb.IS, pb.SM, pb.alg, chunk))) != cudaSuccess)
+      return cuda_fail(ctx, e, "3D scratch");
+    mqp::piv3d_bind_scratch(a, pb.alg, chunk, (char*)ctx->scratch3d.ptr);
+  }
   a.img1 = d1;
   a.img2 = d2;
   a.mask = dmask;

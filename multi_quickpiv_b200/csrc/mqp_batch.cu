@@ -10,8 +10,13 @@
 //                 fused 2D kernel per kernel variant (N, prune, algorithm,
 //                 dtype), whose warps take IAs of all pairs of that variant
 //                 from a single work queue (large and small pairs balance)
-//   side stream   integral volumes of the 3D pairs and their chunked
-//                 K3a/K3b/K3c passes, concurrently with the 2D work
+//   3D lanes      up to four side streams; each 3D pair runs all its steps
+//                 (integral volumes, predictors, passes) on one lane, with
+//                 its own chunk scratch, concurrently with the 2D work and
+//                 the other lanes.  Pairs go to lanes longest first by an
+//                 estimate of their arithmetic (a coarse pass of a few IAs
+//                 cannot fill the GPU alone; lanes let such passes of
+//                 different pairs run side by side).
 //
 // Pass rounds: pair k with L_k passes (refine && multipass > 1, else 1) runs
 // its pass at scale 2^(L_k-1-r) in round r, so every pair's coarse pass comes
@@ -22,6 +27,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cmath>
 #include <functional>
 #include <map>
 #include <string>
@@ -38,11 +44,12 @@ struct mqp_plan {
   mqp_ctx* ctx = nullptr;
   int device = 0;
   DevBuf arena;
-  // enqueue steps: (main stream, side stream) -> MQP_OK or an error code
-  std::vector<std::function<int(cudaStream_t, cudaStream_t)>> ops;
-  cudaStream_t side = nullptr;
+  // enqueue steps: (main stream, 3D lane streams) -> MQP_OK or an error code
+  std::vector<std::function<int(cudaStream_t, const cudaStream_t*)>> ops;
+  std::vector<cudaStream_t> lanes;
+  std::vector<cudaEvent_t> ev_join;
   cudaStream_t cap = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaEvent_t ev_fork = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int64_t total_ia = 0;
@@ -76,7 +83,26 @@ struct ItemPlan {
   std::vector<Level> lev;   // lev[l] = scale 2^l; the first round runs lev[levels-1]
   size_t ii_off[3] = {0, 0, 0};  // IIg2, IIg, II1
   int n_ii = 0;
+  int lane = 0;  // 3D pairs: the side stream all its steps run on
 };
+
+constexpr int LANES3D = 4;
+
+// Rough arithmetic of one 3D pass (FLOPs), for balancing pairs over lanes.
+double cost3d(const Problem& pb) {
+  if (pb.n_ia == 0) return 0.0;
+  if (mqp::direct3d_ok(pb.IS, pb.SM)) {
+    double nf = 1, np = 1;
+    for (int d = 0; d < 3; ++d) {
+      nf *= pb.IS[d];
+      np *= 2 * pb.SM[d] + 1;
+    }
+    return 2.0 * nf * np * (double)pb.n_ia;
+  }
+  const int SS[3] = {pb.IS[0] + 2 * pb.SM[0], pb.IS[1] + 2 * pb.SM[1], pb.IS[2] + 2 * pb.SM[2]};
+  const double N = mqp::piv3d_fft_len(SS);
+  return 7.5 * N * N * N * std::log2(N * N * N) * (double)pb.n_ia;
+}
 
 template <typename T>
 T* at(const mqp_plan* p, size_t off) {
@@ -171,7 +197,33 @@ int mqp_batch_plan_create(mqp_ctx* ctx, const mqp_batch_item* items, int32_t n_i
       }
     }
   }
-  const size_t isc2d_off = ar.take(isc2d), isc3d_off = ar.take(isc3d), scr3d_off = ar.take(scr3d_per + 8 * 256);
+  // 3D pairs to lanes, longest first onto the least loaded lane
+  int n_lanes = 0;
+  {
+    std::vector<std::pair<double, int>> work;
+    for (int k = 0; k < n_items; ++k)
+      if (plan[k].it.ndims == 3) {
+        double c = 0.0;
+        for (const Level& L : plan[k].lev) c += cost3d(L.pb);
+        work.push_back({c, k});
+      }
+    n_lanes = std::min<int>(LANES3D, (int)work.size());
+    std::stable_sort(work.begin(), work.end(), [](const std::pair<double, int>& x, const std::pair<double, int>& y) {
+      return x.first > y.first;
+    });
+    std::vector<double> load(n_lanes, 0.0);
+    for (const auto& w : work) {
+      const int ln = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+      plan[w.second].lane = ln;
+      load[ln] += w.first;
+    }
+  }
+  const size_t isc2d_off = ar.take(isc2d);
+  std::vector<size_t> isc3d_off(n_lanes), scr3d_off(n_lanes);
+  for (int ln = 0; ln < n_lanes; ++ln) {
+    isc3d_off[ln] = ar.take(isc3d);
+    scr3d_off[ln] = ar.take(scr3d_per + 8 * 256);
+  }
 
   // 2D groups per round: one work queue per kernel variant
   struct Group {
@@ -232,10 +284,14 @@ int mqp_batch_plan_create(mqp_ctx* ctx, const mqp_batch_item* items, int32_t n_i
     return cuda_fail(ctx, e, "batch plan scratch");
   }
   e = cudaMemset(P->arena.ptr, 0, ar.size);
-  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&P->side, cudaStreamNonBlocking);
+  P->lanes.assign(n_lanes, nullptr);
+  P->ev_join.assign(n_lanes, nullptr);
+  for (int ln = 0; ln < n_lanes && e == cudaSuccess; ++ln) {
+    e = cudaStreamCreateWithFlags(&P->lanes[ln], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&P->ev_join[ln], cudaEventDisableTiming);
+  }
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&P->cap, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&P->ev_fork, cudaEventDisableTiming);
-  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&P->ev_join, cudaEventDisableTiming);
   if (e != cudaSuccess) {
     mqp_batch_plan_destroy(P);
     return cuda_fail(ctx, e, "batch plan setup");
@@ -297,9 +353,11 @@ int mqp_batch_plan_create(mqp_ctx* ctx, const mqp_batch_item* items, int32_t n_i
     }
 
   // ---- the schedule ----
-  P->ops.push_back([P](cudaStream_t m, cudaStream_t s) {
-    if (cudaEventRecord(P->ev_fork, m) != cudaSuccess || cudaStreamWaitEvent(s, P->ev_fork, 0) != cudaSuccess)
-      return fail(P->ctx, MQP_ERR_CUDA, "batch fork");
+  P->ops.push_back([P](cudaStream_t m, const cudaStream_t* lanes) {
+    if (P->lanes.empty()) return MQP_OK;
+    if (cudaEventRecord(P->ev_fork, m) != cudaSuccess) return fail(P->ctx, MQP_ERR_CUDA, "batch fork");
+    for (size_t ln = 0; ln < P->lanes.size(); ++ln)
+      if (cudaStreamWaitEvent(lanes[ln], P->ev_fork, 0) != cudaSuccess) return fail(P->ctx, MQP_ERR_CUDA, "batch fork");
     return MQP_OK;
   });
   for (int k = 0; k < n_items; ++k) {
@@ -312,10 +370,11 @@ int mqp_batch_plan_create(mqp_ctx* ctx, const mqp_batch_item* items, int32_t n_i
     const int H = (int)ip.it.dims[0], W = (int)ip.it.dims[1], D = d3 ? (int)ip.it.dims[2] : 1;
     double* ii[3] = {at<double>(P, ip.ii_off[0]), n_ii > 1 ? at<double>(P, ip.ii_off[1]) : nullptr,
                      n_ii > 2 ? at<double>(P, ip.ii_off[2]) : nullptr};
-    double* isc = at<double>(P, d3 ? isc3d_off : isc2d_off);
+    double* isc = at<double>(P, d3 ? isc3d_off[ip.lane] : isc2d_off);
+    const int lane = ip.lane;
     P->launches += (int64_t)n_ii * (d3 ? integral_kernels_2d(W) + 1 : integral_kernels_2d(W));
-    P->ops.push_back([=](cudaStream_t m, cudaStream_t s) {
-      cudaStream_t st = d3 ? s : m;
+    P->ops.push_back([=](cudaStream_t m, const cudaStream_t* lanes) {
+      cudaStream_t st = d3 ? lanes[lane] : m;
       const void* src[3] = {i2, i2, i1};
       const bool sq[3] = {true, false, false};
       for (int i = 0; i < n_ii; ++i) {
@@ -348,9 +407,10 @@ int mqp_batch_plan_create(mqp_ctx* ctx, const mqp_batch_item* items, int32_t n_i
       pa.VFc = at<double>(P, C.vf_off);
       pa.pred = at<int32_t>(P, L.pred_off);
       const bool d3 = ip.it.ndims == 3;
+      const int lane = ip.lane;
       P->launches += 1;
-      P->ops.push_back([=](cudaStream_t m, cudaStream_t s) {
-        const cudaError_t e2 = mqp::launch_predictor(pa, d3 ? s : m);
+      P->ops.push_back([=](cudaStream_t m, const cudaStream_t* lanes) {
+        const cudaError_t e2 = mqp::launch_predictor(pa, d3 ? lanes[lane] : m);
         return e2 == cudaSuccess ? MQP_OK : cuda_fail(P->ctx, e2, "batch predictor");
       });
     }
@@ -368,7 +428,7 @@ int mqp_batch_plan_create(mqp_ctx* ctx, const mqp_batch_item* items, int32_t n_i
       b.grab = o.grab;
       b.counter = at<unsigned long long>(P, g.counter_off);
       P->launches += 1;
-      P->ops.push_back([=](cudaStream_t m, cudaStream_t) {
+      P->ops.push_back([=](cudaStream_t m, const cudaStream_t*) {
         std::string err;
         const cudaError_t e2 = mqp::launch_piv2d_batch(b, m, err);
         return e2 == cudaSuccess ? MQP_OK : fail(P->ctx, MQP_ERR_CUDA, "batch 2D launch: " + err);
@@ -382,26 +442,13 @@ int mqp_batch_plan_create(mqp_ctx* ctx, const mqp_batch_item* items, int32_t n_i
       const Problem& pb = L.pb;
       const size_t per = mqp::piv3d_scratch_bytes_per_ia(pb.IS, pb.SM, pb.alg);
       const int64_t chunk = chunk_for(o, per, pb.n_ia);
-      const int SS[3] = {pb.IS[0] + 2 * pb.SM[0], pb.IS[1] + 2 * pb.SM[1], pb.IS[2] + 2 * pb.SM[2]};
-      const int N = mqp::piv3d_fft_len(SS);
-      const bool prune = pb.IS[0] <= N / 2 && pb.IS[1] <= N / 2 && pb.IS[2] <= N / 2;
-      const size_t K3 = N / 2 + 1, NF = prune ? N / 2 : N;
-      const size_t P12 = (size_t)(2 * pb.SM[0] + 1) * (2 * pb.SM[1] + 1), P3 = 2 * pb.SM[2] + 1;
-      const size_t c = (size_t)chunk;
-      char* base = at<char>(P, scr3d_off);
-      const size_t bGz = align256(c * K3 * N * N * sizeof(float2));
-      const size_t bFz = align256(c * K3 * NF * NF * sizeof(float2));
-      const size_t bC = align256(c * K3 * P12 * sizeof(float2));
-      const size_t bC2 = pb.alg == mqp::ALG_MASK_NSQECC ? bC : 0;
-      const size_t bV = align256(c * P12 * P3 * sizeof(float));
       mqp::Piv3dArgs a;
       memset(&a, 0, sizeof(a));
-      a.Gz = (float2*)base;
-      a.Fz = (float2*)(base + bGz);
-      a.C = (float2*)(base + bGz + bFz);
-      a.C2 = bC2 ? (float2*)(base + bGz + bFz + bC) : nullptr;
-      a.V = (float*)(base + bGz + bFz + bC + bC2);
-      a.state = (mqp::IA3State*)(base + bGz + bFz + bC + bC2 + bV);
+      for (int d = 0; d < 3; ++d) {
+        a.IS[d] = pb.IS[d];
+        a.SM[d] = pb.SM[d];
+      }
+      mqp::piv3d_bind_scratch(a, pb.alg, chunk, at<char>(P, scr3d_off[ip.lane]));
       a.img1 = ip.it.img1;
       a.img2 = ip.it.img2;
       a.mask = ip.it.mask;
@@ -430,18 +477,20 @@ int mqp_batch_plan_create(mqp_ctx* ctx, const mqp_batch_item* items, int32_t n_i
       a.mask_threshold = ip.it.params.mask_threshold;
       const int alg = pb.alg;
       const int64_t chunks = (pb.n_ia + chunk - 1) / chunk;
-      P->launches += mqp::direct3d_ok(pb.IS, pb.SM) ? 1 : chunks * (alg == mqp::ALG_MASK_NSQECC ? 5 : 3);
+      P->launches += mqp::direct3d_ok(pb.IS, pb.SM) ? 1 : chunks * (alg == mqp::ALG_MASK_NSQECC ? 7 : 5);
       P->total_ia += pb.n_ia;
-      P->ops.push_back([=](cudaStream_t, cudaStream_t s) {
+      const int lane = ip.lane;
+      P->ops.push_back([=](cudaStream_t, const cudaStream_t* lanes) {
         std::string err;
-        const cudaError_t e2 = mqp::launch_piv3d(a, alg, chunk, s, err);
+        const cudaError_t e2 = mqp::launch_piv3d(a, alg, chunk, lanes[lane], err);
         return e2 == cudaSuccess ? MQP_OK : fail(P->ctx, MQP_ERR_CUDA, "batch 3D launch: " + err);
       });
     }
   }
-  P->ops.push_back([P](cudaStream_t m, cudaStream_t s) {
-    if (cudaEventRecord(P->ev_join, s) != cudaSuccess || cudaStreamWaitEvent(m, P->ev_join, 0) != cudaSuccess)
-      return fail(P->ctx, MQP_ERR_CUDA, "batch join");
+  P->ops.push_back([P](cudaStream_t m, const cudaStream_t* lanes) {
+    for (size_t ln = 0; ln < P->lanes.size(); ++ln)
+      if (cudaEventRecord(P->ev_join[ln], lanes[ln]) != cudaSuccess || cudaStreamWaitEvent(m, P->ev_join[ln], 0) != cudaSuccess)
+        return fail(P->ctx, MQP_ERR_CUDA, "batch join");
     return MQP_OK;
   });
 
@@ -450,7 +499,7 @@ int mqp_batch_plan_create(mqp_ctx* ctx, const mqp_batch_item* items, int32_t n_i
     int rc = e == cudaSuccess ? MQP_OK : cuda_fail(ctx, e, "batch graph capture");
     if (rc == MQP_OK)
       for (auto& op : P->ops)
-        if ((rc = op(P->cap, P->side)) != MQP_OK) break;
+        if ((rc = op(P->cap, P->lanes.data())) != MQP_OK) break;
     cudaGraph_t g = nullptr;
     const cudaError_t e2 = cudaStreamEndCapture(P->cap, &g);
     if (rc == MQP_OK && e2 != cudaSuccess) rc = cuda_fail(ctx, e2, "batch graph capture");
@@ -482,7 +531,7 @@ int mqp_batch_plan_run(mqp_plan* plan, void* stream) {
     return e == cudaSuccess ? MQP_OK : cuda_fail(ctx, e, "batch graph launch");
   }
   for (auto& op : plan->ops) {
-    const int rc = op(s, plan->side);
+    const int rc = op(s, plan->lanes.data());
     if (rc != MQP_OK) return rc;
   }
   return MQP_OK;
@@ -499,13 +548,16 @@ int mqp_batch_plan_info(const mqp_plan* plan, int64_t* total_ia, int64_t* launch
 int mqp_batch_plan_destroy(mqp_plan* plan) {
   if (!plan) return MQP_OK;
   cudaSetDevice(plan->device);
-  if (plan->side) cudaStreamSynchronize(plan->side);
+  for (cudaStream_t ln : plan->lanes)
+    if (ln) cudaStreamSynchronize(ln);
   cudaDeviceSynchronize();
   if (plan->exec) cudaGraphExecDestroy(plan->exec);
   if (plan->graph) cudaGraphDestroy(plan->graph);
   if (plan->ev_fork) cudaEventDestroy(plan->ev_fork);
-  if (plan->ev_join) cudaEventDestroy(plan->ev_join);
-  if (plan->side) cudaStreamDestroy(plan->side);
+  for (cudaEvent_t ev : plan->ev_join)
+    if (ev) cudaEventDestroy(ev);
+  for (cudaStream_t ln : plan->lanes)
+    if (ln) cudaStreamDestroy(ln);
   if (plan->cap) cudaStreamDestroy(plan->cap);
   plan->arena.release();
   delete plan;

@@ -1,9 +1,11 @@
 // sm_100a kernels of the direct (spatial) correlation for small windows, 2D
-// and 3D (see mqp_direct.cuh): one warp per interrogation area.
+// and 3D (see mqp_direct.cuh): one warp per interrogation area, or for the
+// 3D shapes of the register-tiled lag loop one block per interrogation area.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <string>
 
 #include "mqp_direct.cuh"
@@ -247,6 +249,127 @@ __global__ void __launch_bounds__(DWARPS * 32) direct3d_kernel(Piv3dArgs a, int 
     direct3d_ia<ALG, T>(a, ia, ws, lane);
 }
 
+// ---- 3D, register-tiled lags: one block per IA ------------------------------
+constexpr int D3T_MAXT = 256;  // threads of a block (P1 P3 tasks, rounded up to warps)
+constexpr int D3T_RED = 4 * (D3T_MAXT / 32) * 2 + D3T_MAXT / 32;  // reduction words
+
+// Block-wide reductions in a fixed warp order (every thread gets the result).
+__device__ __forceinline__ void block_max_max_sum(double& a, double& b, double& c, double* red, int tid, int nw) {
+  a = dmax(a);
+  b = dmax(b);
+  c = dsum(c);
+  if ((tid & 31) == 0) {
+    red[3 * (tid >> 5)] = a;
+    red[3 * (tid >> 5) + 1] = b;
+    red[3 * (tid >> 5) + 2] = c;
+  }
+  __syncthreads();
+  a = red[0];
+  b = red[1];
+  c = red[2];
+  for (int w = 1; w < nw; ++w) {
+    a = fmax(a, red[3 * w]);
+    b = fmax(b, red[3 * w + 1]);
+    c += red[3 * w + 2];
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ void block_peak(PeakAcc& acc, double* red, int* redi, int tid, int nw) {
+  dpeak(acc.best, acc.bidx);
+  acc.smax = dnmax(acc.smax);
+  acc.ssum = dsum(acc.ssum);
+  if ((tid & 31) == 0) {
+    red[3 * (tid >> 5)] = acc.best;
+    red[3 * (tid >> 5) + 1] = acc.smax;
+    red[3 * (tid >> 5) + 2] = acc.ssum;
+    redi[tid >> 5] = acc.bidx;
+  }
+  __syncthreads();
+  acc.best = red[0];
+  acc.smax = red[1];
+  acc.ssum = red[2];
+  acc.bidx = redi[0];
+  for (int w = 1; w < nw; ++w) {
+    peak_merge(acc.best, acc.bidx, red[3 * w], redi[w]);
+    acc.smax = nmax(acc.smax, red[3 * w + 1]);
+    acc.ssum += red[3 * w + 2];
+  }
+  __syncthreads();
+}
+
+template <int ALG, typename T, int IS2, int P2>
+__device__ __forceinline__ void direct3d_tiled_ia(const Piv3dArgs& a, long long ia, float* ws, double* red, int* redi,
+                                                  int tid, int nt) {
+  constexpr bool MASKED = ALG == ALG_MASK_NSQECC;
+  const int nw = nt >> 5;
+  const int P1 = 2 * a.SM[0] + 1, P3 = 2 * a.SM[2] + 1;
+  const int vol = P1 * P2 * P3;
+  const D3Off o = d3_off(a.IS, a.SM);
+  float* F = ws + o.F;
+  float* G = ws + o.G;
+  float* V = ws + o.V;
+  float* C1 = ws + o.c1;
+  const IAGeom3 g = ia_geom3(a, ia);
+  IA3State s;
+  ia3_means<ALG>(a, g, s.meanF, s.meanG);
+  s.sumF2 = 0.0;
+  s.skip = 0;
+  constexpr int NPASS = MASKED ? 2 : 1;
+  for (int pass = 0; pass < NPASS; ++pass) {
+    const int PASS = MASKED ? (pass == 0 ? PASS_MASKED : PASS_MASK_SQ) : PASS_PLAIN;
+    double vmax = -INFINITY, mmax = -INFINITY, sumsq = 0.0;
+    direct3d_load<T, ALG>(a, g, s, PASS, tid, nt, F, G, vmax, mmax, sumsq, true);
+    if (pass == 0) {
+      block_max_max_sum(vmax, mmax, sumsq, red, tid, nw);  // also orders the loads before the lags
+      s.sumF2 = sumsq;
+      if (skip_test3(a, ALG, vmax, mmax)) {
+        if (tid == 0) {
+          for (int d = 0; d < 3; ++d) a.VF[3 * ia + d] = 0.0;
+          if (a.SN) a.SN[ia] = 0.0;
+        }
+        if (a.planes)
+          for (int i = tid; i < vol; i += nt) a.planes[(ia - a.planes_begin) * (long long)vol + i] = 0.0;
+        return;
+      }
+    } else {
+      __syncthreads();
+    }
+    direct3d_lags_tiled<IS2, P2>(a, tid, nt, F, G, V);
+    __syncthreads();
+    if (MASKED && pass == 0) {
+      for (int i = tid; i < vol; i += nt) C1[i] = V[i];
+      __syncthreads();
+    }
+  }
+  const LagRanges3 R = lag_ranges3(a, g);
+  PeakAcc acc;
+  acc.best = 0.0;
+  acc.bidx = -1;
+  acc.smax = -INFINITY;
+  acc.ssum = 0.0;
+  for (int q = tid; q < vol; q += nt) {
+    const double c = MASKED ? (double)C1[q] : (double)V[q];
+    const double c2 = MASKED ? (double)V[q] : 0.0;
+    const double v = direct3d_sim<ALG>(a, g, s, q, c, c2);
+    V[q] = (float)v;
+    if (a.planes) a.planes[(ia - a.planes_begin) * (long long)vol + q] = v;
+    acc_take3(acc, R, q % P1, (q / P1) % P2, q / (P1 * P2), q, v);
+  }
+  block_peak(acc, red, redi, tid, nw);  // its barriers also publish V
+  if (tid == 0) direct3d_final(a, g, ia, R, V, acc.best, acc.bidx, acc.smax, acc.ssum);
+  __syncthreads();
+}
+
+template <int ALG, typename T, int IS2, int P2>
+__global__ void __launch_bounds__(D3T_MAXT) direct3d_tiled_kernel(Piv3dArgs a, int words) {
+  extern __shared__ float dsm[];
+  double* red = reinterpret_cast<double*>(dsm + words);
+  int* redi = reinterpret_cast<int*>(red + 3 * (D3T_MAXT / 32));
+  for (long long ia = a.ia_begin + blockIdx.x; ia < a.ia_end; ia += gridDim.x)
+    direct3d_tiled_ia<ALG, T, IS2, P2>(a, ia, dsm, red, redi, threadIdx.x, blockDim.x);
+}
+
 // grid: resident blocks of `kern` with `smem` bytes, at most enough for n warps' work
 cudaError_t grid_for(const void* kern, size_t smem, long long n, long long& blocks, std::string& err) {
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -302,8 +425,36 @@ cudaError_t d2_alg(int alg, const Piv2dArgs* single, const Piv2dBatch* batch, cu
   }
 }
 
+template <int ALG, typename T, int IS2, int P2>
+cudaError_t d3t_launch(const Piv3dArgs& a, cudaStream_t s, std::string& err) {
+  const int words = d3_off(a.IS, a.SM).words;
+  const size_t smem = (size_t)(words + D3T_RED) * sizeof(float);
+  const int tasks = (2 * a.SM[0] + 1) * (2 * a.SM[2] + 1);
+  const int nt = std::min(D3T_MAXT, (tasks + 31) / 32 * 32);
+  const void* kern = (const void*)direct3d_tiled_kernel<ALG, T, IS2, P2>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int dev = 0, per_sm = 0;
+  if (e == cudaSuccess) e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, nt, smem);
+  if (e != cudaSuccess || per_sm < 1) {
+    err = "direct 3D kernel does not fit on an SM (shared memory " + std::to_string(smem) + " B)";
+    return e != cudaSuccess ? e : cudaErrorInvalidConfiguration;
+  }
+  const long long n = a.ia_end - a.ia_begin;
+  const long long blocks = std::min<long long>((long long)device_sm_count(dev) * per_sm, n);
+  direct3d_tiled_kernel<ALG, T, IS2, P2><<<(unsigned)blocks, nt, smem, s>>>(a, words);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) err = std::string("direct 3D launch: ") + cudaGetErrorString(e);
+  return e;
+}
+
 template <int ALG, typename T>
 cudaError_t d3_launch(const Piv3dArgs& a, cudaStream_t s, std::string& err) {
+  const int IS2 = a.IS[1], P2 = 2 * a.SM[1] + 1;
+#define MQP_D3_GO(i, p) \
+  if (IS2 == i && P2 == p) return d3t_launch<ALG, T, i, p>(a, s, err);
+  MQP_D3_TILED_SHAPES(MQP_D3_GO)
+#undef MQP_D3_GO
   const int words = d3_off(a.IS, a.SM).words;
   const size_t smem = (size_t)DWARPS * words * sizeof(float);
   long long blocks = 0;

@@ -128,31 +128,48 @@ MQP_HD MQP_FI bool direct3d_ok(const int IS[3], const int SM[3]) {
   return nf <= D3_MAXF && ng <= D3_MAXG && np <= D3_MAXP && nf * np <= (1 << 19);
 }
 
-// Per-warp workspace (4-byte words): F | G | similarity volume | parked first
-// correlation (masked NSQECC), sized for the problem.
+// Workspace of one IA (4-byte words): F | G | similarity volume | parked
+// first correlation (masked NSQECC), sized for the problem.  G's planes along
+// dim 3 are R2 words apart, R2 = S1 S2 padded to P1 modulo 32: the threads of
+// a warp that read G at lags s1 + P1 s3 = 32 consecutive tasks then hit 32
+// distinct banks.
 struct D3Off {
-  int F, G, V, c1, words;
+  int F, G, V, c1, words, R2;
 };
 MQP_HD MQP_FI D3Off d3_off(const int IS[3], const int SM[3]) {
-  int nf = 1, ng = 1, np = 1;
+  int nf = 1, np = 1;
   for (int d = 0; d < 3; ++d) {
     nf *= IS[d];
-    ng *= IS[d] + 2 * SM[d];
     np *= 2 * SM[d] + 1;
   }
+  const int S0 = IS[0] + 2 * SM[0], S1 = IS[1] + 2 * SM[1], S2 = IS[2] + 2 * SM[2];
+  const int P1 = 2 * SM[0] + 1;
   D3Off o;
+  o.R2 = S0 * S1 + (((P1 - S0 * S1) % 32) + 32) % 32;
   o.F = 0;
-  o.G = nf;
-  o.V = nf + ng;
+  o.G = (nf + 3) & ~3;
+  o.V = o.G + o.R2 * S2;
   o.c1 = o.V + np;
-  o.words = (o.c1 + np + 1) & ~1;
+  o.words = (o.c1 + np + 3) & ~3;
   return o;
 }
 
-// F stored x1-fastest (F[x1 + IS1 (x2 + IS2 x3)]), G likewise over the pad.
+// (interSize, lag count) along dim 2 of the register-tiled lag kernel; other
+// shapes take the one-lag-per-lane loop (direct3d_lags).
+#define MQP_D3_TILED_SHAPES(X) X(2, 3) X(4, 5) X(6, 7) X(8, 9) X(8, 5) X(4, 9)
+MQP_HD MQP_FI bool d3_tiled(int IS2, int P2) {
+#define MQP_D3_IS(i, p) if (IS2 == i && P2 == p) return true;
+  MQP_D3_TILED_SHAPES(MQP_D3_IS)
+#undef MQP_D3_IS
+  return false;
+}
+
+// F stored x1-fastest (F[x1 + IS1 (x2 + IS2 x3)]) or, for the tiled kernel,
+// x2-fastest (F[x2 + IS2 (x1 + IS1 x3)]); G x1-fastest over the pad,
+// G[p1 + S1 p2 + R2 p3].
 template <typename T, int ALG>
 MQP_HD MQP_FI void direct3d_load(const Piv3dArgs& a, const IAGeom3& g, const IA3State& s, int PASS, int lane, int nl,
-                                 float* F, float* G, double& vmax, double& mmax, double& sumsq) {
+                                 float* F, float* G, double& vmax, double& mmax, double& sumsq, bool fx2 = false) {
   const long long HW = (long long)a.H * a.W;
   const int I0 = a.IS[0], I1 = a.IS[1], I2 = a.IS[2];
   for (int i = lane; i < I0 * I1 * I2; i += nl) {
@@ -177,9 +194,10 @@ MQP_HD MQP_FI void direct3d_load(const Piv3dArgs& a, const IAGeom3& g, const IA3
     } else {
       w = (float)ldg_px<T>(a.mask, off);
     }
-    F[i] = w;
+    F[fx2 ? x2 + I1 * (x1 + I0 * x3) : i] = w;
   }
   const int S0 = a.IS[0] + 2 * a.SM[0], S1 = a.IS[1] + 2 * a.SM[1], S2 = a.IS[2] + 2 * a.SM[2];
+  const int R2 = d3_off(a.IS, a.SM).R2;
   const float mg = (float)s.meanG;
   for (int i = lane; i < S0 * S1 * S2; i += nl) {
     const int p1 = i % S0, p2 = (i / S0) % S1, p3 = i / (S0 * S1);
@@ -189,14 +207,14 @@ MQP_HD MQP_FI void direct3d_load(const Piv3dArgs& a, const IAGeom3& g, const IA3
       if (ALG == ALG_ZNCC) v = v - mg;
       if (PASS == PASS_MASK_SQ) v = v * v;
     }
-    G[i] = v;
+    G[p1 + S0 * p2 + R2 * p3] = v;
   }
 }
 
 // raw correlation of lag q (s1 fastest) into V[q]
 MQP_HD MQP_FI void direct3d_lags(const Piv3dArgs& a, int lane, int nl, const float* F, const float* G, float* V) {
   const int I0 = a.IS[0], I1 = a.IS[1], I2 = a.IS[2];
-  const int S0 = a.IS[0] + 2 * a.SM[0], S1 = a.IS[1] + 2 * a.SM[1];
+  const int S0 = a.IS[0] + 2 * a.SM[0], R2 = d3_off(a.IS, a.SM).R2;
   const int P1 = 2 * a.SM[0] + 1, P2 = 2 * a.SM[1] + 1, P3 = 2 * a.SM[2] + 1;
   for (int q = lane; q < P1 * P2 * P3; q += nl) {
     const int s1 = q % P1, s2 = (q / P1) % P2, s3 = q / (P1 * P2);
@@ -204,10 +222,50 @@ MQP_HD MQP_FI void direct3d_lags(const Piv3dArgs& a, int lane, int nl, const flo
     for (int x3 = 0; x3 < I2; ++x3)
       for (int x2 = 0; x2 < I1; ++x2) {
         const float* f = F + I0 * (x2 + I1 * x3);
-        const float* gr = G + (s1 + S0 * ((x2 + s2) + S1 * (x3 + s3)));
+        const float* gr = G + (s1 + S0 * (x2 + s2) + R2 * (x3 + s3));
         for (int x1 = 0; x1 < I0; ++x1) acc = fmaf(f[x1], gr[x1], acc);
       }
     V[q] = acc;
+  }
+}
+
+// Register-tiled raw correlation: a task is one (s1, s3) lag pair and owns
+// the P2 lags along dim 2 in registers.  Per (x3, x1) it holds F's IS2 values
+// along dim 2 (x2-fastest F, one broadcast read per value) and streams the
+// SS2 values of its G column, each feeding every lag whose window covers it:
+// IS2 P2 fused multiply-adds per IS2 + SS2 shared-memory reads.  Consecutive
+// tasks read consecutive banks (R2 = P1 modulo 32).  Sums run over x3, x1,
+// then x2 (the one-lag loop sums x3, x2, x1).
+template <int IS2, int P2>
+MQP_HD MQP_FI void direct3d_lags_tiled(const Piv3dArgs& a, int tid, int nt, const float* F, const float* G, float* V) {
+  constexpr int SS2 = IS2 + P2 - 1;
+  const int I0 = a.IS[0], I2 = a.IS[2];
+  const int S0 = a.IS[0] + 2 * a.SM[0], R2 = d3_off(a.IS, a.SM).R2;
+  const int P1 = 2 * a.SM[0] + 1, P3 = 2 * a.SM[2] + 1;
+  for (int task = tid; task < P1 * P3; task += nt) {
+    const int s1 = task % P1, s3 = task / P1;
+    float acc[P2];
+#pragma unroll
+    for (int j = 0; j < P2; ++j) acc[j] = 0.f;
+    for (int x3 = 0; x3 < I2; ++x3) {
+      const float* gz = G + s1 + R2 * (x3 + s3);
+      const float* fz = F + IS2 * I0 * x3;
+      for (int x1 = 0; x1 < I0; ++x1) {
+        float f[IS2];
+#pragma unroll
+        for (int k = 0; k < IS2; ++k) f[k] = fz[IS2 * x1 + k];
+        const float* gp = gz + x1;
+#pragma unroll
+        for (int t = 0; t < SS2; ++t) {
+          const float gv = gp[S0 * t];
+#pragma unroll
+          for (int j = 0; j < P2; ++j)
+            if (t - j >= 0 && t - j < IS2) acc[j] = fmaf(f[t - j], gv, acc[j]);
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < P2; ++j) V[s1 + P1 * (j + P2 * s3)] = acc[j];
   }
 }
 

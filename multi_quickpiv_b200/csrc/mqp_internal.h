@@ -81,6 +81,10 @@ cudaError_t launch_piv2d_big_batch(const Piv2dBatch& b, cudaStream_t s, std::str
 // chunk IAs).
 int piv3d_fft_len(const int SS[3]);
 size_t piv3d_scratch_bytes_per_ia(const int IS[3], const int SM[3], int alg);
+// chunk scratch of the 3D kernels for `chunk` IAs, and Piv3dArgs' scratch
+// pointers bound into it (a.IS / a.SM set)
+size_t piv3d_scratch_bytes(const int IS[3], const int SM[3], int alg, long long chunk);
+void piv3d_bind_scratch(Piv3dArgs& a, int alg, long long chunk, char* base);
 cudaError_t launch_piv3d(const Piv3dArgs& a, int alg, long long chunk, cudaStream_t s, std::string& err);
 
 // Multi-pass refinement: the fine pass's predictor from the coarse vectors.

@@ -14,7 +14,6 @@ namespace mqp {
 namespace {
 
 constexpr int K3A_THREADS = 256;
-constexpr int K3C_THREADS = 256;
 
 __device__ __forceinline__ double warp_sum3(double v) {
 #pragma unroll
@@ -32,10 +31,14 @@ __device__ __forceinline__ double warp_nmax3(double v) {
   return v;
 }
 
-// One block per IA of the chunk; threads walk the IA's lines.
+// Blocks (part, IA): each part walks its contiguous share of the IA's lines.
+// Pass 0 leaves the part's skip maxima and sumF2 in apart; part 0 records the
+// ZNCC means, and k3a_merge_kernel completes the state.
 template <int N, bool FPRUNE, int ALG, typename T>
 __global__ void __launch_bounds__(K3A_THREADS) k3a_kernel(Piv3dArgs a, int pass) {
-  const long long ci = blockIdx.x;
+  constexpr int PARTS = k3a_parts(N);
+  const int part = blockIdx.x;
+  const long long ci = blockIdx.y;
   const IAGeom3 g = ia_geom3(a, a.ia_begin + ci);
   IA3State s;
   if (pass == 0) {
@@ -47,7 +50,8 @@ __global__ void __launch_bounds__(K3A_THREADS) k3a_kernel(Piv3dArgs a, int pass)
   }
   double vmax = -INFINITY, mmax = -INFINITY, sumsq = 0.0;
   const int nl = k3a_lines(a, g);
-  for (int line = threadIdx.x; line < nl; line += K3A_THREADS)
+  const int l0 = (int)((long long)nl * part / PARTS), l1 = (int)((long long)nl * (part + 1) / PARTS);
+  for (int line = l0 + threadIdx.x; line < l1; line += K3A_THREADS)
     k3a_line<N, FPRUNE, T, ALG>(a, g, s, pass, ci, line, vmax, mmax, sumsq);
   if (pass != 0) return;
   __shared__ double red[3][K3A_THREADS / 32];
@@ -67,10 +71,28 @@ __global__ void __launch_bounds__(K3A_THREADS) k3a_kernel(Piv3dArgs a, int pass)
       mmax = fmax(mmax, red[1][w]);
       sumsq += red[2][w];
     }
-    s.sumF2 = sumsq;
-    s.skip = skip_test3(a, ALG, vmax, mmax) ? 1 : 0;
-    a.state[ci] = s;
+    a.apart[ci * PARTS + part] = ReducePart3{vmax, mmax, sumsq};
+    if (part == 0) a.state[ci] = s;
   }
+}
+
+// One thread per IA: its K3a parts in part order -> sumF2 and the skip test.
+template <int N, int ALG>
+__global__ void k3a_merge_kernel(Piv3dArgs a, long long n) {
+  constexpr int PARTS = k3a_parts(N);
+  const long long ci = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (ci >= n) return;
+  const ReducePart3* p = a.apart + ci * PARTS;
+  double vmax = p[0].vmax, mmax = p[0].mmax, sumsq = p[0].sumsq;
+  for (int k = 1; k < PARTS; ++k) {
+    vmax = fmax(vmax, p[k].vmax);
+    mmax = fmax(mmax, p[k].mmax);
+    sumsq += p[k].sumsq;
+  }
+  IA3State s = a.state[ci];
+  s.sumF2 = sumsq;
+  s.skip = skip_test3(a, ALG, vmax, mmax) ? 1 : 0;
+  a.state[ci] = s;
 }
 
 // One block of N threads per (k3, IA) slab.
@@ -96,18 +118,22 @@ __global__ void __launch_bounds__(N) k3b_kernel(Piv3dArgs a, float2* C) {
   k3b_rows2<N, FPRUNE>(ci, k3, t, P1, P2, S, C);
 }
 
-// One block per IA of the chunk.
+// Blocks (part, IA): each part walks its contiguous share of the lag pairs;
+// the part's peak / SN accumulators go to cpart, and k3c_merge_kernel
+// finishes the IA.
 template <int N, int ALG>
 __global__ void __launch_bounds__(K3C_THREADS) k3c_kernel(Piv3dArgs a) {
-  const long long ci = blockIdx.x;
+  const int part = blockIdx.x, parts = gridDim.x;
+  const long long ci = blockIdx.y;
   const int P1 = 2 * a.SM[0] + 1, P2 = 2 * a.SM[1] + 1, P3 = 2 * a.SM[2] + 1;
+  const int q0 = P1 * P2 * part / parts, q1 = P1 * P2 * (part + 1) / parts;
   const IA3State s = a.state[ci];
   if (s.skip) {
-    if (threadIdx.x == 0) k3c_skipped(a, ci);
     if (a.planes) {
       const long long vol = (long long)P1 * P2 * P3;
       double* dst = a.planes + (a.ia_begin + ci - a.planes_begin) * vol;
-      for (long long i = threadIdx.x; i < vol; i += K3C_THREADS) dst[i] = 0.0;
+      for (int q = q0 + threadIdx.x; q < q1; q += K3C_THREADS)
+        for (int s3 = 0; s3 < P3; ++s3) dst[q + (long long)P1 * P2 * s3] = 0.0;
     }
     return;
   }
@@ -118,7 +144,7 @@ __global__ void __launch_bounds__(K3C_THREADS) k3c_kernel(Piv3dArgs a) {
   acc.bidx = -1;
   acc.smax = -INFINITY;
   acc.ssum = 0.0;
-  for (int q = threadIdx.x; q < P1 * P2; q += K3C_THREADS) k3c_pair<N, ALG>(a, g, s, ci, q, P1, P2, P3, R, acc);
+  for (int q = q0 + threadIdx.x; q < q1; q += K3C_THREADS) k3c_pair<N, ALG>(a, g, s, ci, q, P1, P2, P3, R, acc);
   // block merge: (largest value, lowest column-major index), NaN-propagating max, sum
   __shared__ double rb[K3C_THREADS / 32], rs[K3C_THREADS / 32], rm[K3C_THREADS / 32];
   __shared__ int ri[K3C_THREADS / 32];
@@ -139,7 +165,7 @@ __global__ void __launch_bounds__(K3C_THREADS) k3c_kernel(Piv3dArgs a) {
     rm[warp] = smax;
     rs[warp] = ssum;
   }
-  __syncthreads();  // also publishes the similarity volume to thread 0
+  __syncthreads();
   if (threadIdx.x == 0) {
     double b = rb[0], mx = rm[0], sum = rs[0];
     int bi = ri[0];
@@ -148,8 +174,36 @@ __global__ void __launch_bounds__(K3C_THREADS) k3c_kernel(Piv3dArgs a) {
       mx = nmax(mx, rm[w]);
       sum += rs[w];
     }
-    k3c_final(a, g, ci, R, b, bi, mx, sum);
+    PeakPart3 pp;
+    pp.best = b;
+    pp.smax = mx;
+    pp.ssum = sum;
+    pp.bidx = bi;
+    pp.pad_ = 0;
+    a.cpart[ci * gridDim.x + part] = pp;
   }
+}
+
+// One thread per IA: its K3c parts in part order, then the Gaussian fit and
+// SN from the similarity volume (k3c_final).
+template <int N, int ALG>
+__global__ void k3c_merge_kernel(Piv3dArgs a, long long n, int parts) {
+  const long long ci = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (ci >= n) return;
+  if (a.state[ci].skip) {
+    k3c_skipped(a, ci);
+    return;
+  }
+  const PeakPart3* p = a.cpart + ci * parts;
+  double b = p[0].best, mx = p[0].smax, sum = p[0].ssum;
+  int bi = p[0].bidx;
+  for (int k = 1; k < parts; ++k) {
+    peak_merge(b, bi, p[k].best, p[k].bidx);
+    mx = nmax(mx, p[k].smax);
+    sum += p[k].ssum;
+  }
+  const IAGeom3 g = ia_geom3(a, a.ia_begin + ci);
+  k3c_final(a, g, ci, lag_ranges3(a, g), b, bi, mx, sum);
 }
 
 template <int N, bool FPRUNE, int ALG, typename T>
@@ -167,11 +221,15 @@ cudaError_t run_chunks(Piv3dArgs a, long long chunk, cudaStream_t s, std::string
     const long long n = end - c0 < chunk ? end - c0 : chunk;
     a.ia_begin = c0;
     a.ia_end = c0 + n;
+    const unsigned merge_blocks = (unsigned)((n + 127) / 128);
     for (int pass = 0; pass < NPASS; ++pass) {
-      k3a_kernel<N, FPRUNE, ALG, T><<<(unsigned)n, K3A_THREADS, 0, s>>>(a, pass);
+      k3a_kernel<N, FPRUNE, ALG, T><<<dim3(k3a_parts(N), (unsigned)n), K3A_THREADS, 0, s>>>(a, pass);
+      if (pass == 0) k3a_merge_kernel<N, ALG><<<merge_blocks, 128, 0, s>>>(a, n);
       k3b_kernel<N, FPRUNE><<<dim3(L::K3, (unsigned)n), N, smem, s>>>(a, pass == 0 ? a.C : a.C2);
     }
-    k3c_kernel<N, ALG><<<(unsigned)n, K3C_THREADS, 0, s>>>(a);
+    const int cparts = k3c_parts(N, (2 * a.SM[0] + 1) * (2 * a.SM[1] + 1));
+    k3c_kernel<N, ALG><<<dim3(cparts, (unsigned)n), K3C_THREADS, 0, s>>>(a);
+    k3c_merge_kernel<N, ALG><<<merge_blocks, 128, 0, s>>>(a, n, cparts);
     e = cudaGetLastError();
     if (e != cudaSuccess) {
       err = std::string("piv3d launch: ") + cudaGetErrorString(e);
@@ -212,22 +270,64 @@ int piv3d_fft_len(const int SS[3]) {
 
 static bool piv3d_prune(const int IS[3], int N) { return IS[0] <= N / 2 && IS[1] <= N / 2 && IS[2] <= N / 2; }
 
-size_t piv3d_scratch_bytes_per_ia(const int IS[3], const int SM[3], int alg) {
+// Chunk scratch of c IAs: Gz | Fz | C | C2 | V | state | K3a parts | K3c
+// parts, each array 256-byte aligned.
+namespace {
+struct Scr3 {
+  size_t b[8];
+};
+Scr3 scr3(const int IS[3], const int SM[3], int alg, size_t c) {
+  Scr3 r{};
   const int SS[3] = {IS[0] + 2 * SM[0], IS[1] + 2 * SM[1], IS[2] + 2 * SM[2]};
   const int N = piv3d_fft_len(SS);
-  if (N == 0) return 0;
+  if (N == 0) return r;
   const size_t K3 = N / 2 + 1;
   const size_t NF = piv3d_prune(IS, N) ? N / 2 : N;
   const size_t P12 = (size_t)(2 * SM[0] + 1) * (2 * SM[1] + 1);
   const size_t P3 = 2 * SM[2] + 1;
-  const size_t ncorr = alg == ALG_MASK_NSQECC ? 2 : 1;
-  size_t b = 0;
-  b += K3 * N * N * sizeof(float2);        // Gz
-  b += K3 * NF * NF * sizeof(float2);      // Fz
-  b += ncorr * K3 * P12 * sizeof(float2);  // C (and C2)
-  b += P12 * P3 * sizeof(float);           // V
-  b += sizeof(IA3State);
-  return b + 6 * 256;                      // alignment of the six arrays
+  auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  r.b[0] = al(c * K3 * N * N * sizeof(float2));                               // Gz
+  r.b[1] = al(c * K3 * NF * NF * sizeof(float2));                             // Fz
+  r.b[2] = al(c * K3 * P12 * sizeof(float2));                                 // C
+  r.b[3] = alg == ALG_MASK_NSQECC ? r.b[2] : 0;                               // C2
+  r.b[4] = al(c * P12 * P3 * sizeof(float));                                  // V
+  r.b[5] = al(c * sizeof(IA3State));                                          // state
+  r.b[6] = al(c * k3a_parts(N) * sizeof(ReducePart3));                        // K3a parts
+  r.b[7] = al(c * (size_t)k3c_parts(N, (int)P12) * sizeof(PeakPart3));        // K3c parts
+  return r;
+}
+}  // namespace
+
+size_t piv3d_scratch_bytes(const int IS[3], const int SM[3], int alg, long long chunk) {
+  const Scr3 r = scr3(IS, SM, alg, (size_t)chunk);
+  size_t t = 0;
+  for (size_t x : r.b) t += x;
+  return t;
+}
+
+size_t piv3d_scratch_bytes_per_ia(const int IS[3], const int SM[3], int alg) {
+  // one IA's share, with the alignment of the eight arrays
+  return piv3d_scratch_bytes(IS, SM, alg, 1);
+}
+
+void piv3d_bind_scratch(Piv3dArgs& a, int alg, long long chunk, char* base) {
+  const Scr3 r = scr3(a.IS, a.SM, alg, (size_t)chunk);
+  size_t o = 0;
+  a.Gz = (float2*)(base + o);
+  o += r.b[0];
+  a.Fz = (float2*)(base + o);
+  o += r.b[1];
+  a.C = (float2*)(base + o);
+  o += r.b[2];
+  a.C2 = r.b[3] ? (float2*)(base + o) : nullptr;
+  o += r.b[3];
+  a.V = (float*)(base + o);
+  o += r.b[4];
+  a.state = (IA3State*)(base + o);
+  o += r.b[5];
+  a.apart = (ReducePart3*)(base + o);
+  o += r.b[6];
+  a.cpart = (PeakPart3*)(base + o);
 }
 
 cudaError_t launch_piv3d(const Piv3dArgs& a, int alg, long long chunk, cudaStream_t s, std::string& err) {

@@ -38,6 +38,24 @@ struct IA3State {
   int pad_;
 };
 
+// Per-block partial results: K3a's skip maxima and sumF2 over its share of
+// the lines, K3c's peak / SN accumulators over its share of the lag pairs;
+// a merge kernel combines an IA's parts in part order.
+struct ReducePart3 {
+  double vmax, mmax, sumsq;
+};
+struct PeakPart3 {
+  double best, smax, ssum;
+  int bidx, pad_;
+};
+
+// Blocks per IA of K3a (over its z-lines) and K3c (over its lag pairs): at
+// FFT length 128 an IA's lines and lag pairs fill several blocks (the coarse
+// passes that use it have few IAs); shorter lengths keep one block per IA.
+constexpr int K3C_THREADS = 256;
+MQP_HD MQP_FI constexpr int k3a_parts(int N) { return N >= 128 ? 8 : 1; }
+MQP_HD MQP_FI int k3c_parts(int N, int P12) { return N >= 128 ? (P12 + K3C_THREADS - 1) / K3C_THREADS : 1; }
+
 struct Piv3dArgs {
   const void* img1;
   const void* img2;
@@ -64,6 +82,8 @@ struct Piv3dArgs {
   float2* C2;             // masked: mask * G^2 correlation
   float* V;               // [ci][s3][s2][s1] similarity volume
   IA3State* state;        // [ci]
+  ReducePart3* apart;     // [ci][k3a_parts(N)]
+  PeakPart3* cpart;       // [ci][k3c_parts(N, P1 P2)]
 };
 
 template <int N, bool FPRUNE>

@@ -17,10 +17,22 @@
 //             images, 3D chunk scratch, outputs; stream-ordered allocations)
 //             fit the free-memory budget.  Frames of one stream are ordered
 //             by events: request k waits for request k-1's upload.
+//   host side pinned staging and result buffers are allocated when a stream
+//             opens (one per slot); submit copies the frame into staging
+//             outside the server lock, and a finished request's VF/SN move
+//             from pinned memory to host memory the request owns, so requests
+//             whose results are collected late hold no pinned memory and the
+//             worker never waits on a pinned allocation or a large copy.
 //   latency   submit -> result on the host, per request; mqp_server_get_stats
-//             reports p50 / p99 and throughput.
+//             reports p50 / p99 of it and of its two parts (queued: submit ->
+//             issue; running: issue -> done) and throughput.  With the
+//             environment variable MQP_SERVER_TRACE set to a file name, the
+//             server writes every finished request's timeline there (CSV) when
+//             it is destroyed.
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -48,6 +60,32 @@ double now_ms() {
 
 constexpr int RING = 3;
 
+// Pinned host buffers of one size, owned by a stream: staging for its new
+// frames, or downloads of its results.  Buffers go back to `free` when the
+// request that held them finishes; none is released before the server.
+struct HostBufs {
+  size_t n = 0;
+  std::vector<void*> free, all;
+  void* take() {
+    if (free.empty()) return nullptr;
+    void* p = free.back();
+    free.pop_back();
+    return p;
+  }
+  void put(void* p) {
+    if (p) free.push_back(p);
+  }
+  void add(void* p, bool in_use) {
+    all.push_back(p);
+    if (!in_use) free.push_back(p);
+  }
+  void release() {
+    for (void* p : all) cudaFreeHost(p);
+    all.clear();
+    free.clear();
+  }
+};
+
 struct SrvStream {
   int id = 0;
   int ndims = 2;
@@ -63,6 +101,7 @@ struct SrvStream {
   int64_t issued = 0;     // requests issued to a slot
   int64_t done = 0;       // requests completed
   size_t transient = 0;   // device bytes one request allocates while it runs
+  HostBufs stage, res;    // pinned frame staging, pinned result downloads
 };
 
 struct SrvRequest {
@@ -70,8 +109,8 @@ struct SrvRequest {
   int stream = 0;
   int64_t k = 0;        // frame index of the new frame (>= 1)
   void* staging = nullptr;  // pinned copy of the new frame
-  double* vf = nullptr;     // pinned results
-  double* sn = nullptr;
+  double* res = nullptr;    // pinned VF then SN, held while the request runs
+  std::vector<double> vf, sn;  // results, filled when the request finishes
   size_t vf_n = 0, sn_n = 0;
   double t_submit = 0, t_issue = 0, t_done = 0;
   int state = 0;  // 0 queued, 1 running, 2 done, 3 failed
@@ -84,34 +123,6 @@ struct Slot {
   cudaEvent_t done = nullptr;
   uint64_t req = 0;
   bool busy = false;
-};
-
-struct PinnedPool {
-  struct Blk {
-    void* p;
-    size_t n;
-    bool used;
-  };
-  std::vector<Blk> blks;
-  void* get(size_t n) {
-    for (auto& b : blks)
-      if (!b.used && b.n >= n) {
-        b.used = true;
-        return b.p;
-      }
-    void* p = nullptr;
-    if (cudaMallocHost(&p, n) != cudaSuccess) return nullptr;
-    blks.push_back({p, n, true});
-    return p;
-  }
-  void put(void* p) {
-    for (auto& b : blks)
-      if (b.p == p) b.used = false;
-  }
-  void release() {
-    for (auto& b : blks) cudaFreeHost(b.p);
-    blks.clear();
-  }
 };
 
 }  // namespace
@@ -129,9 +140,16 @@ struct mqp_server {
   std::deque<uint64_t> queue;
   uint64_t next_req = 1;
   std::vector<Slot> slots;
-  PinnedPool pinned;
   size_t budget = 0, in_use = 0;
-  std::vector<double> lat;  // completed latencies (ms)
+  std::vector<double> lat, lat_wait, lat_run;  // completed latencies (ms): total, queued, running
+  struct TraceRec {
+    uint64_t id;
+    int stream, slot, state;
+    int64_t k;
+    double t_submit, t_issue, t_done;
+  };
+  std::vector<TraceRec> trace;
+  std::string trace_path;
   double t_first = 0, t_last = 0;
   int64_t ia_done = 0, completed = 0, failed = 0, admitted_overlap = 0;
   std::string last_error;
@@ -245,22 +263,13 @@ std::string issue(mqp_server* S, SrvStream& st, SrvRequest& r, cudaStream_t s) {
     if (!base) {
       err = "transient allocation";
     } else {
-      const int SS[3] = {st.pb.IS[0] + 2 * st.pb.SM[0], st.pb.IS[1] + 2 * st.pb.SM[1], st.pb.IS[2] + 2 * st.pb.SM[2]};
-      const int N = mqp::piv3d_fft_len(SS);
-      const bool prune = st.pb.IS[0] <= N / 2 && st.pb.IS[1] <= N / 2 && st.pb.IS[2] <= N / 2;
-      const size_t K3 = N / 2 + 1, NF = prune ? N / 2 : N, c = (size_t)chunk;
-      const size_t P12 = (size_t)(2 * st.pb.SM[0] + 1) * (2 * st.pb.SM[1] + 1), P3 = 2 * st.pb.SM[2] + 1;
-      const size_t bGz = align256(c * K3 * N * N * sizeof(float2));
-      const size_t bFz = align256(c * K3 * NF * NF * sizeof(float2));
-      const size_t bC = align256(c * K3 * P12 * sizeof(float2));
-      const size_t bV = align256(c * P12 * P3 * sizeof(float));
       mqp::Piv3dArgs a;
       memset(&a, 0, sizeof(a));
-      a.Gz = (float2*)base;
-      a.Fz = (float2*)(base + bGz);
-      a.C = (float2*)(base + bGz + bFz);
-      a.V = (float*)(base + bGz + bFz + bC);
-      a.state = (mqp::IA3State*)(base + bGz + bFz + bC + bV);
+      for (int d = 0; d < 3; ++d) {
+        a.IS[d] = st.pb.IS[d];
+        a.SM[d] = st.pb.SM[d];
+      }
+      mqp::piv3d_bind_scratch(a, st.pb.alg, chunk, base);
       a.img1 = img1;
       a.img2 = img2;
       a.dtype = st.dtype;
@@ -287,10 +296,11 @@ std::string issue(mqp_server* S, SrvStream& st, SrvRequest& r, cudaStream_t s) {
       if ((e = mqp::launch_piv3d(a, st.pb.alg, chunk, s, err)) != cudaSuccess && err.empty()) err = bad(e, "PIV kernels");
     }
   }
-  if (err.empty() && (e = cudaMemcpyAsync(r.vf, dVF, r.vf_n * sizeof(double), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+  if (err.empty() &&
+      (e = cudaMemcpyAsync(r.res, dVF, r.vf_n * sizeof(double), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
     err = bad(e, "VF download");
   if (err.empty() && r.sn_n &&
-      (e = cudaMemcpyAsync(r.sn, dSN, r.sn_n * sizeof(double), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+      (e = cudaMemcpyAsync(r.res + r.vf_n, dSN, r.sn_n * sizeof(double), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
     err = bad(e, "SN download");
   for (void* p : tmp) cudaFreeAsync(p, s);
   return err;
@@ -315,15 +325,22 @@ void worker_loop(mqp_server* S) {
         r.err = std::string("request: ") + cudaGetErrorString(q);
         ++S->failed;
       } else {
+        r.vf.assign(r.res, r.res + r.vf_n);
+        if (r.sn_n) r.sn.assign(r.res + r.vf_n, r.res + r.vf_n + r.sn_n);
         r.state = 2;
         S->lat.push_back(r.t_done - r.t_submit);
+        S->lat_wait.push_back(r.t_issue - r.t_submit);
+        S->lat_run.push_back(r.t_done - r.t_issue);
         S->ia_done += st.pb.n_ia;
         ++S->completed;
         S->t_last = r.t_done;
       }
-      S->pinned.put(r.staging);
+      st.stage.put(r.staging);
+      st.res.put(r.res);
       r.staging = nullptr;
+      r.res = nullptr;
       S->in_use -= request_bytes(st);
+      if (!S->trace_path.empty()) S->trace.push_back({r.id, r.stream, (int)i, r.state, r.k, r.t_submit, r.t_issue, r.t_done});
       st.done += 1;
       sl.busy = false;
       progress = true;
@@ -347,6 +364,19 @@ void worker_loop(mqp_server* S) {
         ++it;
         continue;
       }
+      // the stream's pinned result buffers number the slots and at most
+      // slots - 1 requests run now, so one is free (allocated only if
+      // open_stream could not make them all)
+      r.res = (double*)st.res.take();
+      if (!r.res) {
+        void* h = nullptr;
+        if (cudaMallocHost(&h, st.res.n) != cudaSuccess) {
+          ++it;
+          continue;
+        }
+        st.res.add(h, true);
+        r.res = (double*)h;
+      }
       Slot& sl = S->slots[free_slot];
       int busy = 0;
       for (auto& o : S->slots) busy += o.busy;
@@ -365,8 +395,10 @@ void worker_loop(mqp_server* S) {
         r.t_done = now_ms();
         ++S->failed;
         st.done += 1;
-        S->pinned.put(r.staging);
+        st.stage.put(r.staging);
+        st.res.put(r.res);
         r.staging = nullptr;
+        r.res = nullptr;
       } else {
         r.state = 1;
         r.slot = free_slot;
@@ -417,6 +449,7 @@ int mqp_server_create(int device, const mqp_server_options* opt, mqp_server** ou
     uint64_t keep = UINT64_MAX;
     cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
   }
+  if (const char* tp = getenv("MQP_SERVER_TRACE")) S->trace_path = tp;
   S->slots.resize(S->opt.slots);
   for (auto& sl : S->slots) {
     if ((e = cudaStreamCreateWithFlags(&sl.s, cudaStreamNonBlocking)) != cudaSuccess ||
@@ -490,6 +523,32 @@ int mqp_server_open_stream(mqp_server* S, const void* first_frame, int dtype, in
     return srv_fail(S, e == cudaErrorMemoryAllocation ? MQP_ERR_OOM : MQP_ERR_CUDA,
                     std::string("open stream: ") + cudaGetErrorString(e));
   }
+  // pinned staging for new frames and result buffers, one per slot (staging
+  // bounded to 256 MiB per stream; further frames in flight allocate more)
+  st.res.n = (size_t)std::max<int64_t>(st.pb.n_ia, 1) * (st.ndims + (st.p.computeSN ? 1 : 0)) * sizeof(double);
+  st.stage.n = st.frame_bytes;
+  const size_t n_stage = std::max<size_t>(1, std::min<size_t>(S->slots.size(), ((size_t)256 << 20) / st.frame_bytes));
+  for (size_t i = 0; i < S->slots.size() + n_stage; ++i) {
+    HostBufs& hb = i < S->slots.size() ? st.res : st.stage;
+    void* h = nullptr;
+    if (cudaMallocHost(&h, hb.n) != cudaSuccess) break;  // allocated again on demand
+    hb.add(h, false);
+  }
+  // grow the device pool now to hold every slot running a request of this
+  // stream: growing it later (two large 3D requests meeting for the first
+  // time) would stall the worker inside the allocation for tens of ms
+  {
+    const size_t need = request_bytes(st);
+    std::vector<void*> warm;
+    for (size_t i = 0; i < S->slots.size() && S->in_use + (i + 1) * need <= S->budget; ++i) {
+      void* d = nullptr;
+      if (cudaMallocAsync(&d, need, S->slots[0].s) != cudaSuccess) break;
+      warm.push_back(d);
+    }
+    for (void* d : warm) cudaFreeAsync(d, S->slots[0].s);
+    cudaStreamSynchronize(S->slots[0].s);
+    cudaGetLastError();
+  }
   S->streams[st.id] = st;
   *stream_id = S->next_stream++;
   return MQP_OK;
@@ -497,26 +556,48 @@ int mqp_server_open_stream(mqp_server* S, const void* first_frame, int dtype, in
 
 int mqp_server_submit(mqp_server* S, int32_t stream_id, const void* frame, uint64_t* request_id) {
   if (!S || !frame || !request_id) return srv_fail(S, MQP_ERR_INVALID, "null argument");
+  SrvRequest r;
+  size_t frame_bytes = 0;
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    auto f = S->streams.find(stream_id);
+    if (f == S->streams.end()) return srv_fail(S, MQP_ERR_NOT_FOUND, "unknown stream " + std::to_string(stream_id));
+    const SrvStream& st = f->second;
+    frame_bytes = st.frame_bytes;
+    r.vf_n = (size_t)std::max<int64_t>(st.pb.n_ia, 1) * st.ndims;
+    r.sn_n = st.p.computeSN ? (size_t)std::max<int64_t>(st.pb.n_ia, 1) : 0;
+    r.staging = f->second.stage.take();
+  }
+  // a pinned allocation (all staging buffers in flight) and the frame copy
+  // run without the lock, so the worker keeps admitting and completing
+  if (!r.staging) {
+    void* h = nullptr;
+    if (cudaMallocHost(&h, frame_bytes) != cudaSuccess) return srv_fail(S, MQP_ERR_OOM, "pinned staging");
+    r.staging = h;
+    std::lock_guard<std::mutex> lk(S->mu);
+    auto f = S->streams.find(stream_id);
+    if (f == S->streams.end()) {
+      cudaFreeHost(h);
+      return srv_fail(S, MQP_ERR_NOT_FOUND, "unknown stream " + std::to_string(stream_id));
+    }
+    f->second.stage.add(h, true);
+  }
+  memcpy(r.staging, frame, frame_bytes);
   std::lock_guard<std::mutex> lk(S->mu);
   auto f = S->streams.find(stream_id);
-  if (f == S->streams.end()) return srv_fail(S, MQP_ERR_NOT_FOUND, "unknown stream " + std::to_string(stream_id));
+  if (f == S->streams.end()) {
+    return srv_fail(S, MQP_ERR_NOT_FOUND, "unknown stream " + std::to_string(stream_id));
+  }
   SrvStream& st = f->second;
-  SrvRequest r;
   r.id = S->next_req++;
   r.stream = stream_id;
   r.k = ++st.submitted;
-  r.vf_n = (size_t)std::max<int64_t>(st.pb.n_ia, 1) * st.ndims;
-  r.sn_n = st.p.computeSN ? (size_t)std::max<int64_t>(st.pb.n_ia, 1) : 0;
-  r.staging = S->pinned.get(st.frame_bytes);
-  r.vf = (double*)S->pinned.get(r.vf_n * sizeof(double));
-  r.sn = r.sn_n ? (double*)S->pinned.get(r.sn_n * sizeof(double)) : nullptr;
-  if (!r.staging || !r.vf || (r.sn_n && !r.sn)) return srv_fail(S, MQP_ERR_OOM, "pinned staging");
-  memcpy(r.staging, frame, st.frame_bytes);
   r.t_submit = now_ms();
   if (S->t_first == 0) S->t_first = r.t_submit;
-  S->reqs[r.id] = r;
-  S->queue.push_back(r.id);
-  *request_id = r.id;
+  const uint64_t id = r.id;
+  S->reqs[id] = std::move(r);
+  S->queue.push_back(id);
+  *request_id = id;
   S->cv_work.notify_one();
   return MQP_OK;
 }
@@ -538,12 +619,10 @@ int mqp_server_result(mqp_server* S, uint64_t request_id, int32_t wait_ms, doubl
   if (r.state == 3) {
     rc = srv_fail(S, MQP_ERR_CUDA, r.err);
   } else {
-    if (VF) memcpy(VF, r.vf, r.vf_n * sizeof(double));
-    if (SN && r.sn) memcpy(SN, r.sn, r.sn_n * sizeof(double));
+    if (VF) memcpy(VF, r.vf.data(), r.vf_n * sizeof(double));
+    if (SN && r.sn_n) memcpy(SN, r.sn.data(), r.sn_n * sizeof(double));
     if (latency_ms) *latency_ms = r.t_done - r.t_submit;
   }
-  S->pinned.put(r.vf);
-  if (r.sn) S->pinned.put(r.sn);
   S->reqs.erase(request_id);
   return rc;
 }
@@ -552,9 +631,19 @@ int mqp_server_get_stats(mqp_server* S, mqp_server_stats* out) {
   if (!S || !out) return MQP_ERR_INVALID;
   std::lock_guard<std::mutex> lk(S->mu);
   memset(out, 0, sizeof(*out));
-  std::vector<double> l = S->lat;
-  std::sort(l.begin(), l.end());
-  auto pct = [&](double q) { return l.empty() ? 0.0 : l[std::min(l.size() - 1, (size_t)(q * (l.size() - 1) + 0.5))]; };
+  auto sorted = [](std::vector<double> v) {
+    std::sort(v.begin(), v.end());
+    return v;
+  };
+  const std::vector<double> l = sorted(S->lat), lw = sorted(S->lat_wait), lr = sorted(S->lat_run);
+  auto pct_of = [](const std::vector<double>& v, double q) {
+    return v.empty() ? 0.0 : v[std::min(v.size() - 1, (size_t)(q * (v.size() - 1) + 0.5))];
+  };
+  auto pct = [&](double q) { return pct_of(l, q); };
+  out->wait_p50_ms = pct_of(lw, 0.50);
+  out->wait_p99_ms = pct_of(lw, 0.99);
+  out->run_p50_ms = pct_of(lr, 0.50);
+  out->run_p99_ms = pct_of(lr, 0.99);
   out->completed = S->completed;
   out->failed = S->failed;
   out->queued = (int64_t)S->queue.size();
@@ -577,6 +666,9 @@ int mqp_server_reset_stats(mqp_server* S) {
   if (!S) return MQP_ERR_INVALID;
   std::lock_guard<std::mutex> lk(S->mu);
   S->lat.clear();
+  S->lat_wait.clear();
+  S->lat_run.clear();
+  S->trace.clear();
   S->ia_done = 0;
   S->completed = 0;
   S->failed = 0;
@@ -594,6 +686,16 @@ int mqp_server_destroy(mqp_server* S) {
   }
   S->cv_work.notify_all();
   if (S->worker.joinable()) S->worker.join();
+  if (!S->trace_path.empty()) {
+    if (FILE* f = fopen(S->trace_path.c_str(), "w")) {
+      fprintf(f, "request,stream,frame,slot,state,t_submit_ms,t_issue_ms,t_done_ms\n");
+      const double t0 = S->trace.empty() ? 0.0 : S->trace.front().t_submit;
+      for (const auto& t : S->trace)
+        fprintf(f, "%llu,%d,%lld,%d,%d,%.3f,%.3f,%.3f\n", (unsigned long long)t.id, t.stream, (long long)t.k, t.slot,
+                t.state, t.t_submit - t0, t.t_issue - t0, t.t_done - t0);
+      fclose(f);
+    }
+  }
   cudaSetDevice(S->device);
   for (auto& sl : S->slots) {
     if (sl.s) cudaStreamSynchronize(sl.s);
@@ -607,8 +709,9 @@ int mqp_server_destroy(mqp_server* S) {
       if (st.ii[i]) cudaFree(st.ii[i]);
       if (st.ready[i]) cudaEventDestroy(st.ready[i]);
     }
+    st.stage.release();
+    st.res.release();
   }
-  S->pinned.release();
   delete S;
   return MQP_OK;
 }

@@ -1,7 +1,8 @@
 // Host emulation of the direct (spatial) correlation kernels for small
 // windows (test infrastructure, not part of the product library): the same
-// per-lane functions as direct2d_kernel / direct3d_kernel (mqp_direct.cuh),
-// run as one lane covering every element, with sequential reductions.
+// per-lane functions as direct2d_kernel / direct3d_kernel /
+// direct3d_tiled_kernel (mqp_direct.cuh), run as one lane covering every
+// element, with sequential reductions.
 #include <math.h>
 #include <stdint.h>
 #include <string.h>
@@ -100,7 +101,8 @@ static void emu_d3_ia(const Piv3dArgs& a, long long ia, std::vector<float>& ws) 
   for (int pass = 0; pass < NPASS; ++pass) {
     const int PASS = MASKED ? (pass == 0 ? PASS_MASKED : PASS_MASK_SQ) : PASS_PLAIN;
     double vmax = -INFINITY, mmax = -INFINITY, sumsq = 0.0;
-    direct3d_load<T, ALG>(a, g, s, PASS, 0, 1, F, G, vmax, mmax, sumsq);
+    const bool tiled = d3_tiled(a.IS[1], P2);
+    direct3d_load<T, ALG>(a, g, s, PASS, 0, 1, F, G, vmax, mmax, sumsq, tiled);
     if (pass == 0) {
       s.sumF2 = sumsq;
       if (skip_test3(a, ALG, vmax, mmax)) {
@@ -110,7 +112,11 @@ static void emu_d3_ia(const Piv3dArgs& a, long long ia, std::vector<float>& ws) 
         return;
       }
     }
-    direct3d_lags(a, 0, 1, F, G, V);
+    if (!tiled) direct3d_lags(a, 0, 1, F, G, V);
+#define MQP_D3_EMU(i, p) \
+  else if (a.IS[1] == i && P2 == p) direct3d_lags_tiled<i, p>(a, 0, 1, F, G, V);
+    MQP_D3_TILED_SHAPES(MQP_D3_EMU)
+#undef MQP_D3_EMU
     if (MASKED && pass == 0)
       for (int i = 0; i < vol; ++i) C1[i] = V[i];
   }

@@ -130,7 +130,9 @@ def test_emulated_3d_threshold_skip(emu):
 @pytest.mark.parametrize("alg", ["fft", "zncc", "nsqecc"])
 @pytest.mark.parametrize("cfg", [((24, 20, 20), (4, 4, 4), (2, 2, 2), (4, 4, 4)),
                                  ((28, 24, 24), (8, 8, 8), (4, 4, 4), (8, 8, 8)),
-                                 ((24, 24, 20), (6, 4, 8), (2, 3, 2), (6, 5, 6))], ids=["is4", "is8", "aniso"])
+                                 ((24, 24, 20), (6, 4, 8), (2, 3, 2), (6, 5, 6)),
+                                 ((26, 22, 24), (6, 2, 4), (3, 1, 2), (4, 3, 4))],
+                         ids=["is4", "is8", "aniso", "tiled_aniso"])
 def test_emulated_3d_direct_small_windows(emu, alg, cfg):
     """Small 3D windows take the direct (spatial) correlation kernel."""
     shape, IS, SM, st = cfg

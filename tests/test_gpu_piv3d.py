@@ -163,3 +163,45 @@ def test_shear_workload_512x512x256_fftcc(gpu):
     assert np.abs(np.median(inner[2]) - shift[2]) < 0.05
     u1 = np.median(inner[0], axis=(0, 1))
     assert np.max(np.abs(u1 - (shift[0] + shear * zc))) < 0.1
+
+
+DIRECT_CASES = [((24, 20, 20), (4, 4, 4), (2, 2, 2), (4, 4, 4)),
+                ((28, 24, 24), (8, 8, 8), (4, 4, 4), (8, 8, 8)),
+                ((24, 24, 20), (6, 4, 8), (2, 3, 2), (6, 5, 6)),
+                ((26, 22, 24), (6, 2, 4), (3, 1, 2), (4, 3, 4))]
+
+
+@pytest.mark.parametrize("alg", ["fft", "zncc", "nsqecc"])
+@pytest.mark.parametrize("cfg", DIRECT_CASES, ids=["is4", "is8", "aniso", "tiled_aniso"])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_piv3d_direct_small_windows(alg, cfg, dtype, gpu):
+    """Search windows up to 16 per axis: the direct (spatial) correlation,
+    register-tiled for (interSize, lags) along dim 2 in the tiled list (4/5,
+    8/9, 2/3) and one lag per lane otherwise (4/7)."""
+    shape, IS, SM, st = cfg
+    i1, i2, _ = synth.pair_3d_shear(shape=shape, seed_stream=37, shift=(1.3, -0.7, 0.9), shear=0.0, dtype=dtype)
+    po = O.set_piv_parameters(corr_alg=alg, interSize=IS, searchMargin=SM, step=st, computeSN=True)
+    po.ndims = 3
+    VFo, SNo, Co = O.piv_single_pass(i1, i2, po, keep_corr=True)
+    pp = _params(alg, IS, SM, st)
+    VF, SN = PIV(i1, i2, pp)
+    planes = correlation_planes(i1, i2, pp)
+    _check(VF, SN, planes, VFo, SNo, Co, shape, IS, SM, st)
+
+
+def test_piv3d_direct_masked(gpu):
+    shape, IS, SM, st = (24, 24, 24), (8, 8, 8), (4, 4, 4), (4, 4, 4)
+    i1, i2, _ = synth.pair_3d_shear(shape=shape, seed_stream=38, shift=(1.2, 0.4, -0.8), shear=0.0,
+                                    dtype=np.float64)
+    mask = synth.ellipse_mask(np.random.default_rng(6), shape, cover=0.7)
+    po = O.set_piv_parameters(interSize=IS, searchMargin=SM, step=st, computeSN=True)
+    po.ndims = 3
+    VFo, SNo, Co = O.piv_single_pass(i1, i2, po, mask=mask, keep_corr=True)
+    pp = _params("nsqecc", IS, SM, st)
+    VF, SN = PIV(i1, i2, mask, pp)
+    planes = correlation_planes(i1, i2, pp, mask=mask)
+    sparse = mask_coverage(mask, shape, IS, st) < 0.25
+    worst, near_tie = compare_planes(planes, Co, shape, IS, SM, st, skip=sparse)
+    assert worst <= MASK_PLANE_RTOL, worst
+    bad = (np.abs(VF - VFo) > VF_ATOL).any(axis=0) & ~near_tie & ~sparse
+    assert not bad.any(), np.abs(VF - VFo).max()
