@@ -155,9 +155,13 @@ MQP_API int mqp_profile_read(mqp_ctx* ctx, mqp_profile* out);
  * plans take no such knobs).  Results never depend on these values.
  *   MQP_TUNE_CHUNK3D         IAs per chunk of the 3D path (0 = from the budget)
  *   MQP_TUNE_CHUNK3D_BUDGET  device bytes of 3D chunk scratch (default 1 GiB)
+ *   MQP_TUNE_HOST_PIECES     column pieces of the pipelined host-array 2D path
+ *                            (single pass, images >= 1024 columns; default 3,
+ *                            1 = copy everything first; at most 16)
  * Returns MQP_ERR_INVALID for an unknown key or a negative value. */
 #define MQP_TUNE_CHUNK3D 1
 #define MQP_TUNE_CHUNK3D_BUDGET 2
+#define MQP_TUNE_HOST_PIECES 3
 MQP_API int mqp_set_tuning(mqp_ctx* ctx, int key, int64_t value);
 
 /*

@@ -22,7 +22,7 @@ MQP_ERR_BUSY = -6
 MQP_ERR_NOT_FOUND = -7
 
 MQP_FFTCC, MQP_ZNCC, MQP_NSQECC, MQP_MASK_NSQECC = 0, 1, 2, 3
-MQP_TUNE_CHUNK3D, MQP_TUNE_CHUNK3D_BUDGET = 1, 2
+MQP_TUNE_CHUNK3D, MQP_TUNE_CHUNK3D_BUDGET, MQP_TUNE_HOST_PIECES = 1, 2, 3
 MQP_F32, MQP_F64 = 0, 1
 
 # every symbol declared in include/mqp.h, with its ctypes signature
@@ -212,6 +212,10 @@ class Context:
         """IAs per 3D chunk (0: as many as budget_bytes of scratch hold)."""
         check(self.lib.mqp_set_tuning(self.handle, MQP_TUNE_CHUNK3D, int(ias)), self.handle)
         check(self.lib.mqp_set_tuning(self.handle, MQP_TUNE_CHUNK3D_BUDGET, int(budget_bytes)), self.handle)
+
+    def set_host_pieces(self, pieces: int = 3):
+        """Column pieces of the pipelined host-array 2D path (1: copy first)."""
+        check(self.lib.mqp_set_tuning(self.handle, MQP_TUNE_HOST_PIECES, int(pieces)), self.handle)
 
     def close(self):
         if getattr(self, "handle", None):

@@ -49,6 +49,12 @@ int mqp_destroy(mqp_ctx* ctx) {
                     &ctx->scratch3d, &ctx->passVF[0], &ctx->passVF[1], &ctx->post_in, &ctx->post_mask,
                     &ctx->post_out, &ctx->post_outf, &ctx->post_mask_out, &ctx->post_scratch})
     b->release();
+  for (cudaStream_t st : {ctx->in_stream, ctx->out_stream})
+    if (st) {
+      cudaStreamSynchronize(st);
+      cudaStreamDestroy(st);
+    }
+  for (cudaEvent_t ev : ctx->pipe_ev) cudaEventDestroy(ev);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return MQP_OK;
@@ -76,17 +82,47 @@ namespace mqp_host {
 
 size_t elem_size(int dtype) { return dtype == MQP_F64 ? 8 : 4; }
 
-// Enqueue one pass of the 2D path on device arrays.
-int run_pass_2d(mqp_ctx* ctx, const Problem& pb, const mqp_params* p, const void* d1, const void* d2,
-                const void* dmask, const void* dskip, int dtype, double* dVF, double* dSN,
-                const int32_t* dpred, double* dplanes, int64_t ia_begin, int64_t ia_end, cudaStream_t s) {
+// The integral images a 2D pass needs (ctx buffers), over image columns
+// [x0, x1): the whole image, or one piece of the host-array pipeline.
+static int integrals_2d(mqp_ctx* ctx, const Problem& pb, const void* d1, const void* d2, int dtype, cudaStream_t s,
+                        int x0, int x1) {
   const int H = (int)pb.dims[0], W = (int)pb.dims[1];
-  const int SS1 = pb.IS[0] + 2 * pb.SM[0], SS2 = pb.IS[1] + 2 * pb.SM[1];
-  if (mqp::piv2d_fft_len(SS1, SS2) == 0)
-    return fail(ctx, MQP_ERR_UNSUPPORTED, "2D search window (interSize + 2 searchMargin) above 128 is not supported");
-  if (pb.IS[0] > H || pb.IS[1] > W) return MQP_OK;  // empty vector field
+  if (pb.alg != mqp::ALG_NSQECC && pb.alg != mqp::ALG_ZNCC) return MQP_OK;
   const size_t ii_bytes = (size_t)(H + 1) * (size_t)(W + 1) * sizeof(double);
   cudaError_t e;
+  // one totals area per integral image: a piece's row offsets read the
+  // totals its integral's earlier pieces left
+  const size_t tb = mqp::integral2d_scratch_bytes(H, W);
+  if ((e = ctx->iscratch.ensure(3 * tb)) != cudaSuccess) return cuda_fail(ctx, e, "integral scratch");
+  const bool whole = x0 == 0 && x1 == W;
+  auto integral = [&](const void* img, bool sq, double* out, int k) {
+    double* isc = (double*)((char*)ctx->iscratch.ptr + k * tb);
+    return whole ? mqp::launch_integral2d(img, dtype, H, W, sq, out, isc, s)
+                 : mqp::launch_integral2d_cols(img, dtype, H, W, x0, x1, sq, out, isc, s);
+  };
+  {
+    ProfileScope ps(ctx, s, 0, 0);
+    if ((e = ctx->IIg2.ensure(ii_bytes)) != cudaSuccess) return cuda_fail(ctx, e, "integral buffer");
+    if ((e = integral(d2, true, (double*)ctx->IIg2.ptr, 0)) != cudaSuccess)
+      return cuda_fail(ctx, e, "integral image of img2^2");
+  }
+  if (pb.alg == mqp::ALG_ZNCC) {
+    ProfileScope ps(ctx, s, 0, 0);
+    if ((e = ctx->IIg.ensure(ii_bytes)) != cudaSuccess) return cuda_fail(ctx, e, "integral buffer");
+    if ((e = ctx->II1.ensure(ii_bytes)) != cudaSuccess) return cuda_fail(ctx, e, "integral buffer");
+    if ((e = integral(d2, false, (double*)ctx->IIg.ptr, 1)) != cudaSuccess)
+      return cuda_fail(ctx, e, "integral image of img2");
+    if ((e = integral(d1, false, (double*)ctx->II1.ptr, 2)) != cudaSuccess)
+      return cuda_fail(ctx, e, "integral image of img1");
+  }
+  return MQP_OK;
+}
+
+// Kernel arguments of a 2D pass over IAs [ia_begin, ia_end) (integral images
+// from the ctx buffers).
+static mqp::Piv2dArgs args_2d(mqp_ctx* ctx, const Problem& pb, const mqp_params* p, const void* d1, const void* d2,
+                              const void* dmask, const void* dskip, int dtype, double* dVF, double* dSN,
+                              const int32_t* dpred, double* dplanes, int64_t ia_begin, int64_t ia_end) {
   mqp::Piv2dArgs a;
   memset(&a, 0, sizeof(a));
   a.img1 = d1;
@@ -95,26 +131,8 @@ int run_pass_2d(mqp_ctx* ctx, const Problem& pb, const mqp_params* p, const void
   a.mask_skip = dskip;
   a.mask_threshold = p->mask_threshold;
   a.dtype = dtype;
-  if (pb.alg == mqp::ALG_NSQECC || pb.alg == mqp::ALG_ZNCC) {
-    if ((e = ctx->iscratch.ensure(mqp::integral2d_scratch_bytes(H, W))) != cudaSuccess)
-      return cuda_fail(ctx, e, "integral scratch");
-  }
-  double* isc = (double*)ctx->iscratch.ptr;
-  if (pb.alg == mqp::ALG_NSQECC || pb.alg == mqp::ALG_ZNCC) {
-    ProfileScope ps(ctx, s, 0, 0);
-    if ((e = ctx->IIg2.ensure(ii_bytes)) != cudaSuccess) return cuda_fail(ctx, e, "integral buffer");
-    if ((e = mqp::launch_integral2d(d2, dtype, H, W, true, (double*)ctx->IIg2.ptr, isc, s)) != cudaSuccess)
-      return cuda_fail(ctx, e, "integral image of img2^2");
-    a.IIg2 = (const double*)ctx->IIg2.ptr;
-  }
+  if (pb.alg == mqp::ALG_NSQECC || pb.alg == mqp::ALG_ZNCC) a.IIg2 = (const double*)ctx->IIg2.ptr;
   if (pb.alg == mqp::ALG_ZNCC) {
-    ProfileScope ps(ctx, s, 0, 0);
-    if ((e = ctx->IIg.ensure(ii_bytes)) != cudaSuccess) return cuda_fail(ctx, e, "integral buffer");
-    if ((e = ctx->II1.ensure(ii_bytes)) != cudaSuccess) return cuda_fail(ctx, e, "integral buffer");
-    if ((e = mqp::launch_integral2d(d2, dtype, H, W, false, (double*)ctx->IIg.ptr, isc, s)) != cudaSuccess)
-      return cuda_fail(ctx, e, "integral image of img2");
-    if ((e = mqp::launch_integral2d(d1, dtype, H, W, false, (double*)ctx->II1.ptr, isc, s)) != cudaSuccess)
-      return cuda_fail(ctx, e, "integral image of img1");
     a.IIg = (const double*)ctx->IIg.ptr;
     a.II1 = (const double*)ctx->II1.ptr;
   }
@@ -122,8 +140,8 @@ int run_pass_2d(mqp_ctx* ctx, const Problem& pb, const mqp_params* p, const void
   a.VF = dVF;
   a.SN = dSN;
   a.planes = dplanes;
-  a.H = H;
-  a.W = W;
+  a.H = (int)pb.dims[0];
+  a.W = (int)pb.dims[1];
   a.IS1 = pb.IS[0];
   a.IS2 = pb.IS[1];
   a.SM1 = pb.SM[0];
@@ -136,13 +154,33 @@ int run_pass_2d(mqp_ctx* ctx, const Problem& pb, const mqp_params* p, const void
   a.ia_end = ia_end;
   a.threshold = p->threshold;
   a.computeSN = dSN != nullptr;
+  return a;
+}
+
+static int launch_2d(mqp_ctx* ctx, const mqp::Piv2dArgs& a, int alg, cudaStream_t s) {
   std::string err;
+  cudaError_t e;
   {
-    ProfileScope ps(ctx, s, 1, ia_end - ia_begin);
-    e = mqp::launch_piv2d(a, pb.alg, s, err);
+    ProfileScope ps(ctx, s, 1, a.ia_end - a.ia_begin);
+    e = mqp::launch_piv2d(a, alg, s, err);
   }
   if (e != cudaSuccess) return fail(ctx, e == cudaErrorInvalidValue ? MQP_ERR_UNSUPPORTED : MQP_ERR_CUDA, err);
   return MQP_OK;
+}
+
+// Enqueue one pass of the 2D path on device arrays.
+int run_pass_2d(mqp_ctx* ctx, const Problem& pb, const mqp_params* p, const void* d1, const void* d2,
+                const void* dmask, const void* dskip, int dtype, double* dVF, double* dSN,
+                const int32_t* dpred, double* dplanes, int64_t ia_begin, int64_t ia_end, cudaStream_t s) {
+  const int H = (int)pb.dims[0], W = (int)pb.dims[1];
+  const int SS1 = pb.IS[0] + 2 * pb.SM[0], SS2 = pb.IS[1] + 2 * pb.SM[1];
+  if (mqp::piv2d_fft_len(SS1, SS2) == 0)
+    return fail(ctx, MQP_ERR_UNSUPPORTED, "2D search window (interSize + 2 searchMargin) above 128 is not supported");
+  if (pb.IS[0] > H || pb.IS[1] > W) return MQP_OK;  // empty vector field
+  int rc = integrals_2d(ctx, pb, d1, d2, dtype, s, 0, W);
+  if (rc != MQP_OK) return rc;
+  return launch_2d(ctx, args_2d(ctx, pb, p, d1, d2, dmask, dskip, dtype, dVF, dSN, dpred, dplanes, ia_begin, ia_end),
+                   pb.alg, s);
 }
 
 size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
@@ -331,6 +369,112 @@ int mqp_piv_device(mqp_ctx* ctx, const void* d_img1, const void* d_img2, const v
                          nullptr, 0, -1);
 }
 
+// One 2D pass from host arrays, pipelined: the images (and masks) go up in
+// pieces of whole columns on a copy-in stream (column-major: a piece is one
+// contiguous range, the pieces growing geometrically); the compute stream
+// waits for each piece, builds its
+// integral columns and runs the IA columns whose windows lie within the
+// columns received so far; their vectors go down on a copy-out stream while
+// later pieces compute.  Every IA and every integral value is computed as in
+// the one-shot path, so the results are identical.
+static int host_pipelined_2d(mqp_ctx* ctx, const Problem& pb, const mqp_params* p, const void* img1,
+                             const void* img2, const void* mask, const void* mask_skip, int dtype, double* VF,
+                             double* SN) {
+  const int H = (int)pb.dims[0], W = (int)pb.dims[1];
+  const int64_t vf1 = pb.vf[0], vf2 = pb.vf[1];
+  const size_t es = elem_size(dtype), colb = (size_t)H * es;
+  const int PIPE_PIECES = ctx->host_pieces;
+  cudaError_t e;
+  if (!ctx->in_stream && (e = cudaStreamCreateWithFlags(&ctx->in_stream, cudaStreamNonBlocking)) != cudaSuccess)
+    return cuda_fail(ctx, e, "copy stream");
+  if (!ctx->out_stream && (e = cudaStreamCreateWithFlags(&ctx->out_stream, cudaStreamNonBlocking)) != cudaSuccess)
+    return cuda_fail(ctx, e, "copy stream");
+  while (ctx->pipe_ev.size() < 2 * PIPE_PIECES + 1) {
+    cudaEvent_t ev;
+    if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return cuda_fail(ctx, e, "event");
+    ctx->pipe_ev.push_back(ev);
+  }
+  const size_t ib = colb * (size_t)W;
+  for (DevBuf* b : {&ctx->img1, &ctx->img2})
+    if ((e = b->ensure(ib)) != cudaSuccess) return cuda_fail(ctx, e, "image buffer");
+  if (mask && (e = ctx->mask.ensure(ib)) != cudaSuccess) return cuda_fail(ctx, e, "mask buffer");
+  if (mask_skip && (e = ctx->mask_skip.ensure(ib)) != cudaSuccess) return cuda_fail(ctx, e, "mask buffer");
+  const size_t nvf = (size_t)pb.n_ia;
+  if ((e = ctx->VF.ensure(nvf * 2 * sizeof(double))) != cudaSuccess) return cuda_fail(ctx, e, "VF buffer");
+  double* dSN = nullptr;
+  if (SN) {
+    if ((e = ctx->SN.ensure(nvf * sizeof(double))) != cudaSuccess) return cuda_fail(ctx, e, "SN buffer");
+    dSN = (double*)ctx->SN.ptr;
+  }
+  double* dVF = (double*)ctx->VF.ptr;
+  cudaStream_t s = ctx->stream, si = ctx->in_stream, so = ctx->out_stream;
+  // the compute stream's earlier work (another call's kernels reading the
+  // buffers) precedes this call's copies
+  if ((e = cudaEventRecord(ctx->pipe_ev[2 * PIPE_PIECES], s)) != cudaSuccess ||
+      (e = cudaStreamWaitEvent(si, ctx->pipe_ev[2 * PIPE_PIECES], 0)) != cudaSuccess)
+    return cuda_fail(ctx, e, "pipeline order");
+  // IA column v2 reads image columns below need(v2) (IA window, search window
+  // data, and the integral columns of its lag windows)
+  mqp::Piv2dArgs g0 = args_2d(ctx, pb, p, nullptr, nullptr, nullptr, nullptr, dtype, nullptr, nullptr, nullptr,
+                              nullptr, 0, 0);
+  auto need = [&](int64_t v2) {
+    const mqp::IAGeom g = mqp::ia_geom(g0, 0, (int)v2);
+    return std::max(g.ir2 + pb.IS[1], g.g02 + g.hi2);
+  };
+  int64_t done_cols = 0;  // IA columns launched
+  struct Out {
+    int k;
+    size_t a0, n;  // IAs [a0, a0 + n) finished by piece k
+  };
+  std::vector<Out> outs;
+  int x0 = 0;
+  for (int k = 0; k < PIPE_PIECES; ++k) {
+    // geometric pieces (each twice the last): a small first piece starts
+    // the kernels early, and the later copies hide behind the compute
+    const int64_t den = ((int64_t)1 << PIPE_PIECES) - 1, num = ((int64_t)1 << (k + 1)) - 1;
+    int x1 = k == PIPE_PIECES - 1 ? W : (int)(((int64_t)W * num / den + 63) / 64 * 64);
+    if (x1 > W) x1 = W;
+    if (x1 <= x0) continue;
+    const size_t off = colb * (size_t)x0, len = colb * (size_t)(x1 - x0);
+    const void* src[4] = {img1, img2, mask, mask_skip};
+    DevBuf* dst[4] = {&ctx->img1, &ctx->img2, &ctx->mask, &ctx->mask_skip};
+    for (int i = 0; i < 4; ++i)
+      if (src[i] && (e = cudaMemcpyAsync((char*)dst[i]->ptr + off, (const char*)src[i] + off, len,
+                                         cudaMemcpyHostToDevice, si)) != cudaSuccess)
+        return cuda_fail(ctx, e, "copy images");
+    if ((e = cudaEventRecord(ctx->pipe_ev[k], si)) != cudaSuccess || (e = cudaStreamWaitEvent(s, ctx->pipe_ev[k], 0)) != cudaSuccess)
+      return cuda_fail(ctx, e, "pipeline order");
+    int rc = integrals_2d(ctx, pb, ctx->img1.ptr, ctx->img2.ptr, dtype, s, x0, x1);
+    if (rc != MQP_OK) return rc;
+    int64_t c1 = done_cols;
+    while (c1 < vf2 && (x1 == W || need(c1) <= x1)) ++c1;
+    if (c1 > done_cols) {
+      rc = launch_2d(ctx, args_2d(ctx, pb, p, ctx->img1.ptr, ctx->img2.ptr, mask ? ctx->mask.ptr : nullptr,
+                                  mask_skip ? ctx->mask_skip.ptr : nullptr, dtype, dVF, dSN, nullptr, nullptr,
+                                  vf1 * done_cols, vf1 * c1),
+                     pb.alg, s);
+      if (rc != MQP_OK) return rc;
+      if ((e = cudaEventRecord(ctx->pipe_ev[PIPE_PIECES + k], s)) != cudaSuccess) return cuda_fail(ctx, e, "pipeline order");
+      outs.push_back({k, (size_t)(vf1 * done_cols), (size_t)(vf1 * (c1 - done_cols))});
+      done_cols = c1;
+    }
+    x0 = x1;
+  }
+  // downloads after every upload is enqueued: a copy into pageable memory
+  // returns only when done, and would hold back the next piece's upload
+  for (const auto& o : outs) {
+    if ((e = cudaStreamWaitEvent(so, ctx->pipe_ev[PIPE_PIECES + o.k], 0)) != cudaSuccess)
+      return cuda_fail(ctx, e, "pipeline order");
+    if (VF && (e = cudaMemcpyAsync(VF + 2 * o.a0, dVF + 2 * o.a0, 2 * o.n * sizeof(double), cudaMemcpyDeviceToHost, so)) != cudaSuccess)
+      return cuda_fail(ctx, e, "copy VF");
+    if (SN && (e = cudaMemcpyAsync(SN + o.a0, dSN + o.a0, o.n * sizeof(double), cudaMemcpyDeviceToHost, so)) != cudaSuccess)
+      return cuda_fail(ctx, e, "copy SN");
+  }
+  if ((e = cudaStreamSynchronize(so)) != cudaSuccess) return cuda_fail(ctx, e, "PIV kernels");
+  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(ctx, e, "PIV kernels");
+  return MQP_OK;
+}
+
 static int host_roundtrip(mqp_ctx* ctx, const void* img1, const void* img2, const void* mask,
                           const void* mask_skip, int dtype, int ndims, const int64_t dims[3],
                           const mqp_params* p, double* VF, double* SN, int64_t vf_dims_out[3],
@@ -345,6 +489,11 @@ static int host_roundtrip(mqp_ctx* ctx, const void* img1, const void* img2, cons
   if (rc != MQP_OK) return rc;
   if (vf_dims_out)
     for (int d = 0; d < 3; ++d) vf_dims_out[d] = pb.vf[d];
+  // one 2D pass into host arrays: pipelined copies (wide images only)
+  if (ndims == 2 && !planes && !(p->refine && p->multipass > 1) && pb.n_ia > 0 && pb.dims[1] >= 1024 &&
+      ctx->host_pieces > 1 &&
+      mqp::piv2d_fft_len(pb.IS[0] + 2 * pb.SM[0], pb.IS[1] + 2 * pb.SM[1]) != 0)
+    return host_pipelined_2d(ctx, pb, p, img1, img2, mask, mask_skip, dtype, VF, SN);
   size_t npx = 1;
   for (int d = 0; d < ndims; ++d) npx *= (size_t)dims[d];
   const size_t ib = npx * elem_size(dtype);
@@ -641,6 +790,10 @@ int mqp_set_tuning(mqp_ctx* ctx, int key, int64_t value) {
   switch (key) {
     case MQP_TUNE_CHUNK3D: ctx->chunk3d = value; return MQP_OK;
     case MQP_TUNE_CHUNK3D_BUDGET: ctx->chunk3d_budget = value > 0 ? (size_t)value : ((size_t)1 << 30); return MQP_OK;
+    case MQP_TUNE_HOST_PIECES:
+      if (value < 1 || value > 16) return fail(ctx, MQP_ERR_INVALID, "host pieces must be in [1, 16]");
+      ctx->host_pieces = (int)value;
+      return MQP_OK;
     default: return fail(ctx, MQP_ERR_INVALID, "unknown tuning key " + std::to_string(key));
   }
 }

@@ -47,6 +47,10 @@ struct mqp_ctx {
   mqp_host::DevBuf img1, img2, mask, mask_skip, II1, IIg, IIg2, VF, SN, pred, planes, status, iscratch, scratch3d;
   mqp_host::DevBuf passVF[2];  // vectors of the coarse passes of a multi-pass refinement
   mqp_host::DevBuf post_in, post_mask, post_out, post_outf, post_mask_out, post_scratch;
+  // host-array 2D path: copy-in and copy-out streams, events of its pieces
+  cudaStream_t in_stream = nullptr, out_stream = nullptr;
+  std::vector<cudaEvent_t> pipe_ev;
+  int host_pieces = 3;
   // 3D path: IAs per chunk (0 = sized from chunk3d_budget bytes of scratch)
   int64_t chunk3d = 0;
   size_t chunk3d_budget = (size_t)1 << 30;

@@ -19,6 +19,10 @@ namespace mqp {
 // integral2d_scratch_bytes(H, W) bytes of per-chunk totals.
 cudaError_t launch_integral2d(const void* img, int dtype, int H, int W, bool square,
                               double* out, double* scratch, cudaStream_t s);
+// the integral columns of image columns [x0, x1) (x0 a multiple of 64, x1 one
+// or W) after those of columns < x0: a piece of launch_integral2d's result
+cudaError_t launch_integral2d_cols(const void* img, int dtype, int H, int W, int x0, int x1, bool square,
+                                   double* out, double* scratch, cudaStream_t s);
 size_t integral2d_scratch_bytes(int H, int W);
 
 // The same for a column-major H x W x D volume: out is (H+1) x (W+1) x (D+1),

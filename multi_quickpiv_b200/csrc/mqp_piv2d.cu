@@ -19,15 +19,16 @@ namespace mqp {
 // zero first row.
 // blockIdx.y selects one of a batch of planes (the z slices of a volume):
 // input plane z starts at img + z*in_plane, its output at out + z*out_plane.
+// Output columns [cb, ce) of the (W+1)-column integral.
 template <typename T, bool SQ>
 __global__ void integral_cols_kernel(const T* __restrict__ img, int H, int W, double* __restrict__ out,
-                                     long long in_plane, long long out_plane) {
+                                     long long in_plane, long long out_plane, int cb, int ce) {
   const int warps = blockDim.x >> 5;
   const int lane = threadIdx.x & 31;
   const long long ld = (long long)H + 1;
   img += in_plane * blockIdx.y;
   out += out_plane * blockIdx.y;
-  for (int c = blockIdx.x * warps + (threadIdx.x >> 5); c <= W; c += gridDim.x * warps) {
+  for (int c = cb + blockIdx.x * warps + (threadIdx.x >> 5); c < ce; c += gridDim.x * warps) {
     double* o = out + ld * c;
     if (c == 0) {
       for (int r = lane; r <= H; r += 32) o[r] = 0.0;
@@ -62,10 +63,10 @@ __global__ void integral_cols_kernel(const T* __restrict__ img, int H, int W, do
 constexpr int ICHUNK = 64;
 
 __global__ void integral_rows_chunk_kernel(int H, int W, double* __restrict__ out, double* __restrict__ totals,
-                                           long long out_plane, long long tot_plane) {
+                                           long long out_plane, long long tot_plane, int k0) {
   const long long ld = (long long)H + 1;
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  const int k = blockIdx.y;
+  const int k = blockIdx.y + k0;
   if (r > H) return;
   out += out_plane * blockIdx.z;
   totals += tot_plane * blockIdx.z;
@@ -91,12 +92,13 @@ __global__ void integral_rows_chunk_kernel(int H, int W, double* __restrict__ ou
 }
 
 // pass 3: every chunk k > 0 adds the sum of the totals of chunks 0..k-1
+// (chunks k0 + blockIdx.y, k0 >= 1)
 __global__ void integral_rows_offset_kernel(int H, int W, double* __restrict__ out,
                                             const double* __restrict__ totals, long long out_plane,
-                                            long long tot_plane) {
+                                            long long tot_plane, int k0) {
   const long long ld = (long long)H + 1;
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  const int k = blockIdx.y + 1;
+  const int k = blockIdx.y + k0;
   if (r > H) return;
   out += out_plane * blockIdx.z;
   totals += tot_plane * blockIdx.z;
@@ -121,27 +123,35 @@ __global__ void integral_zscan_kernel(long long plane, int D, double* __restrict
 }
 
 // 2D exclusive-prefix integrals of `planes` consecutive H x W planes of img,
-// plane z written to out + z*out_plane.
+// plane z written to out + z*out_plane: the integral columns that image
+// columns [x0, x1) complete (x0 a multiple of 64, x1 one or W), after those
+// of image columns < x0.  Piece by piece or at once, every value comes out
+// of the same sums in the same order.
 static cudaError_t integral_planes(const void* img, int dtype, int H, int W, int planes, bool square, double* out,
-                                   long long out_plane, double* scratch, cudaStream_t s) {
+                                   long long out_plane, double* scratch, cudaStream_t s, int x0 = 0, int x1 = -1) {
+  if (x1 < 0) x1 = W;
+  if (x0 % ICHUNK != 0 || x1 <= x0 || x1 > W || (x1 % ICHUNK != 0 && x1 != W)) return cudaErrorInvalidValue;
   const int threads = 256;
-  const int blocks = (W + 1 + 7) / 8 < 4096 ? (W + 1 + 7) / 8 : 4096;
+  const int cb = x0 == 0 ? 0 : x0 + 1, ce = x1 + 1;  // integral column c sums image columns < c
+  const int blocks = (ce - cb + 7) / 8 < 4096 ? (ce - cb + 7) / 8 : 4096;
   const long long in_plane = (long long)H * W;
   const dim3 gc(blocks, planes);
   if (dtype == 0) {
-    if (square) integral_cols_kernel<float, true><<<gc, threads, 0, s>>>((const float*)img, H, W, out, in_plane, out_plane);
-    else integral_cols_kernel<float, false><<<gc, threads, 0, s>>>((const float*)img, H, W, out, in_plane, out_plane);
+    if (square) integral_cols_kernel<float, true><<<gc, threads, 0, s>>>((const float*)img, H, W, out, in_plane, out_plane, cb, ce);
+    else integral_cols_kernel<float, false><<<gc, threads, 0, s>>>((const float*)img, H, W, out, in_plane, out_plane, cb, ce);
   } else {
-    if (square) integral_cols_kernel<double, true><<<gc, threads, 0, s>>>((const double*)img, H, W, out, in_plane, out_plane);
-    else integral_cols_kernel<double, false><<<gc, threads, 0, s>>>((const double*)img, H, W, out, in_plane, out_plane);
+    if (square) integral_cols_kernel<double, true><<<gc, threads, 0, s>>>((const double*)img, H, W, out, in_plane, out_plane, cb, ce);
+    else integral_cols_kernel<double, false><<<gc, threads, 0, s>>>((const double*)img, H, W, out, in_plane, out_plane, cb, ce);
   }
   const int chunks = (W + ICHUNK - 1) / ICHUNK;
+  const int k0 = x0 / ICHUNK, k1 = (x1 + ICHUNK - 1) / ICHUNK;  // row chunks of this piece
   const long long tot_plane = (long long)(H + 1) * (chunks + 1);
-  const dim3 g1((H + 1 + 127) / 128, chunks, planes);
-  integral_rows_chunk_kernel<<<g1, 128, 0, s>>>(H, W, out, scratch, out_plane, tot_plane);
-  if (chunks > 1) {
-    const dim3 g2((H + 1 + 127) / 128, chunks - 1, planes);
-    integral_rows_offset_kernel<<<g2, 128, 0, s>>>(H, W, out, scratch, out_plane, tot_plane);
+  const dim3 g1((H + 1 + 127) / 128, k1 - k0, planes);
+  integral_rows_chunk_kernel<<<g1, 128, 0, s>>>(H, W, out, scratch, out_plane, tot_plane, k0);
+  const int ko = k0 > 1 ? k0 : 1;
+  if (k1 > ko) {
+    const dim3 g2((H + 1 + 127) / 128, k1 - ko, planes);
+    integral_rows_offset_kernel<<<g2, 128, 0, s>>>(H, W, out, scratch, out_plane, tot_plane, ko);
   }
   return cudaGetLastError();
 }
@@ -149,6 +159,11 @@ static cudaError_t integral_planes(const void* img, int dtype, int H, int W, int
 cudaError_t launch_integral2d(const void* img, int dtype, int H, int W, bool square, double* out,
                               double* scratch, cudaStream_t s) {
   return integral_planes(img, dtype, H, W, 1, square, out, 0, scratch, s);
+}
+
+cudaError_t launch_integral2d_cols(const void* img, int dtype, int H, int W, int x0, int x1, bool square,
+                                   double* out, double* scratch, cudaStream_t s) {
+  return integral_planes(img, dtype, H, W, 1, square, out, 0, scratch, s, x0, x1);
 }
 
 cudaError_t launch_integral3d(const void* img, int dtype, int H, int W, int D, bool square, double* out,

@@ -138,3 +138,29 @@ def test_piv2d_big_window_masked(gpu):
     assert worst <= MASK_PLANE_RTOL, worst
     bad = (np.abs(VF - VFo) > VF_ATOL).any(axis=0) & ~near_tie
     assert not bad.any(), np.abs(VF - VFo).max()
+
+
+@pytest.mark.parametrize("alg", ["fft", "zncc", "nsqecc", "masked"])
+@pytest.mark.parametrize("cfg", [((32, 32), (16, 16), (16, 16)), ((64, 48), (32, 24), (24, 32)),
+                                 ((8, 8), (4, 4), (8, 8))], ids=["n64", "n128", "direct"])
+def test_host_pipeline_matches_device(alg, cfg, gpu):
+    """Host arrays at least 1024 columns wide take the pipelined copy path
+    (column pieces, per-piece integral columns and IA columns); its VF and SN
+    equal the device-array path's bit for bit."""
+    import torch
+    IS, SM, st = cfg
+    g = np.random.default_rng(61)
+    shape = (300, 1300)  # 1300 columns: the last piece ends off a 64-column boundary
+    i1 = (g.random(shape) * 100).astype(np.float32)
+    i2 = np.roll(i1, (2, -3), axis=(0, 1)) + g.normal(0, 2, shape).astype(np.float32)
+    masks = []
+    if alg == "masked":
+        masks = [synth.ellipse_mask(np.random.default_rng(7), shape, cover=0.6).astype(np.float32)]
+    pp = setPIVParameters(corr_alg="nsqecc" if alg == "masked" else alg, interSize=IS, searchMargin=SM, step=st,
+                          computeSN=True)
+    VF, SN = PIV(i1, i2, *masks, pp)
+    dev = torch.device("cuda", 0)
+    tm = [torch.from_numpy(m).to(dev) for m in masks]
+    VFd, SNd = PIV(torch.from_numpy(i1).to(dev), torch.from_numpy(i2).to(dev), *tm, pp)
+    assert np.array_equal(VF, VFd.cpu().numpy(), equal_nan=True)
+    assert np.array_equal(SN, SNd.cpu().numpy(), equal_nan=True)
