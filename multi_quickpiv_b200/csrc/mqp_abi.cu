@@ -475,6 +475,99 @@ static int host_pipelined_2d(mqp_ctx* ctx, const Problem& pb, const mqp_params* 
   return MQP_OK;
 }
 
+// The 3D FFTCC pass (no integral volumes) pipelined the same way over z: the
+// volumes go up in geometrically growing pieces of whole z-planes (each one
+// contiguous range); the IA layers (vector-field z indices) whose windows the
+// received planes cover run while later planes copy.
+static int host_pipelined_3d(mqp_ctx* ctx, const Problem& pb, const mqp_params* p, const void* img1,
+                             const void* img2, int dtype, double* VF, double* SN) {
+  const int H = (int)pb.dims[0], W = (int)pb.dims[1], D = (int)pb.dims[2];
+  const int64_t layer = pb.vf[0] * pb.vf[1], vf3 = pb.vf[2];
+  const size_t planeb = (size_t)H * (size_t)W * elem_size(dtype);
+  const int PIECES = ctx->host_pieces;
+  cudaError_t e;
+  if (!ctx->in_stream && (e = cudaStreamCreateWithFlags(&ctx->in_stream, cudaStreamNonBlocking)) != cudaSuccess)
+    return cuda_fail(ctx, e, "copy stream");
+  if (!ctx->out_stream && (e = cudaStreamCreateWithFlags(&ctx->out_stream, cudaStreamNonBlocking)) != cudaSuccess)
+    return cuda_fail(ctx, e, "copy stream");
+  while (ctx->pipe_ev.size() < 2 * (size_t)PIECES + 1) {
+    cudaEvent_t ev;
+    if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return cuda_fail(ctx, e, "event");
+    ctx->pipe_ev.push_back(ev);
+  }
+  const size_t ib = planeb * (size_t)D;
+  for (DevBuf* b : {&ctx->img1, &ctx->img2})
+    if ((e = b->ensure(ib)) != cudaSuccess) return cuda_fail(ctx, e, "image buffer");
+  const size_t nvf = (size_t)pb.n_ia;
+  if ((e = ctx->VF.ensure(nvf * 3 * sizeof(double))) != cudaSuccess) return cuda_fail(ctx, e, "VF buffer");
+  double* dSN = nullptr;
+  if (SN) {
+    if ((e = ctx->SN.ensure(nvf * sizeof(double))) != cudaSuccess) return cuda_fail(ctx, e, "SN buffer");
+    dSN = (double*)ctx->SN.ptr;
+  }
+  double* dVF = (double*)ctx->VF.ptr;
+  cudaStream_t s = ctx->stream, si = ctx->in_stream, so = ctx->out_stream;
+  if ((e = cudaEventRecord(ctx->pipe_ev[2 * PIECES], s)) != cudaSuccess ||
+      (e = cudaStreamWaitEvent(si, ctx->pipe_ev[2 * PIECES], 0)) != cudaSuccess)
+    return cuda_fail(ctx, e, "pipeline order");
+  mqp::Piv3dArgs g0;
+  memset(&g0, 0, sizeof(g0));
+  g0.H = H;
+  g0.W = W;
+  g0.D = D;
+  for (int d = 0; d < 3; ++d) {
+    g0.IS[d] = pb.IS[d];
+    g0.SM[d] = pb.SM[d];
+    g0.st[d] = pb.st[d];
+    g0.vf[d] = (int)pb.vf[d];
+  }
+  auto need = [&](int64_t v3) {  // z-planes below this cover IA layer v3
+    const mqp::IAGeom3 g = mqp::ia_geom3(g0, layer * v3);
+    return std::max(g.ir[2] + pb.IS[2], g.g0[2] + g.hi[2]);
+  };
+  struct Out {
+    int k;
+    size_t a0, n;
+  };
+  std::vector<Out> outs;
+  int64_t done = 0;  // IA layers launched
+  int z0 = 0;
+  for (int k = 0; k < PIECES; ++k) {
+    const int64_t den = ((int64_t)1 << PIECES) - 1, num = ((int64_t)1 << (k + 1)) - 1;
+    int z1 = k == PIECES - 1 ? D : (int)((int64_t)D * num / den);
+    if (z1 > D) z1 = D;
+    if (z1 <= z0) continue;
+    const size_t off = planeb * (size_t)z0, len = planeb * (size_t)(z1 - z0);
+    if ((e = cudaMemcpyAsync((char*)ctx->img1.ptr + off, (const char*)img1 + off, len, cudaMemcpyHostToDevice, si)) != cudaSuccess ||
+        (e = cudaMemcpyAsync((char*)ctx->img2.ptr + off, (const char*)img2 + off, len, cudaMemcpyHostToDevice, si)) != cudaSuccess)
+      return cuda_fail(ctx, e, "copy volumes");
+    if ((e = cudaEventRecord(ctx->pipe_ev[k], si)) != cudaSuccess || (e = cudaStreamWaitEvent(s, ctx->pipe_ev[k], 0)) != cudaSuccess)
+      return cuda_fail(ctx, e, "pipeline order");
+    int64_t v1 = done;
+    while (v1 < vf3 && (z1 == D || need(v1) <= z1)) ++v1;
+    if (v1 > done) {
+      const int rc = run_pass_3d(ctx, pb, p, ctx->img1.ptr, ctx->img2.ptr, nullptr, nullptr, dtype, dVF, dSN, nullptr,
+                                 nullptr, layer * done, layer * v1, s);
+      if (rc != MQP_OK) return rc;
+      if ((e = cudaEventRecord(ctx->pipe_ev[PIECES + k], s)) != cudaSuccess) return cuda_fail(ctx, e, "pipeline order");
+      outs.push_back({k, (size_t)(layer * done), (size_t)(layer * (v1 - done))});
+      done = v1;
+    }
+    z0 = z1;
+  }
+  for (const auto& o : outs) {
+    if ((e = cudaStreamWaitEvent(so, ctx->pipe_ev[PIECES + o.k], 0)) != cudaSuccess)
+      return cuda_fail(ctx, e, "pipeline order");
+    if (VF && (e = cudaMemcpyAsync(VF + 3 * o.a0, dVF + 3 * o.a0, 3 * o.n * sizeof(double), cudaMemcpyDeviceToHost, so)) != cudaSuccess)
+      return cuda_fail(ctx, e, "copy VF");
+    if (SN && (e = cudaMemcpyAsync(SN + o.a0, dSN + o.a0, o.n * sizeof(double), cudaMemcpyDeviceToHost, so)) != cudaSuccess)
+      return cuda_fail(ctx, e, "copy SN");
+  }
+  if ((e = cudaStreamSynchronize(so)) != cudaSuccess) return cuda_fail(ctx, e, "PIV kernels");
+  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(ctx, e, "PIV kernels");
+  return MQP_OK;
+}
+
 static int host_roundtrip(mqp_ctx* ctx, const void* img1, const void* img2, const void* mask,
                           const void* mask_skip, int dtype, int ndims, const int64_t dims[3],
                           const mqp_params* p, double* VF, double* SN, int64_t vf_dims_out[3],
@@ -494,6 +587,9 @@ static int host_roundtrip(mqp_ctx* ctx, const void* img1, const void* img2, cons
       ctx->host_pieces > 1 &&
       mqp::piv2d_fft_len(pb.IS[0] + 2 * pb.SM[0], pb.IS[1] + 2 * pb.SM[1]) != 0)
     return host_pipelined_2d(ctx, pb, p, img1, img2, mask, mask_skip, dtype, VF, SN);
+  if (ndims == 3 && !planes && !(p->refine && p->multipass > 1) && pb.n_ia > 0 && pb.alg == mqp::ALG_FFTCC &&
+      !mask && pb.dims[2] >= 64 && ctx->host_pieces > 1)
+    return host_pipelined_3d(ctx, pb, p, img1, img2, dtype, VF, SN);
   size_t npx = 1;
   for (int d = 0; d < ndims; ++d) npx *= (size_t)dims[d];
   const size_t ib = npx * elem_size(dtype);

@@ -34,8 +34,10 @@ __device__ __forceinline__ double warp_nmax3(double v) {
 // Blocks (part, IA): each part walks its contiguous share of the IA's lines.
 // Pass 0 leaves the part's skip maxima and sumF2 in apart; part 0 records the
 // ZNCC means, and k3a_merge_kernel completes the state.
+// Two blocks per SM (16 warps): registers capped at 128 (a few bytes of
+// spill at length 64) instead of one 147-register block.
 template <int N, bool FPRUNE, int ALG, typename T>
-__global__ void __launch_bounds__(K3A_THREADS) k3a_kernel(Piv3dArgs a, int pass) {
+__global__ void __launch_bounds__(K3A_THREADS, 2) k3a_kernel(Piv3dArgs a, int pass) {
   constexpr int PARTS = k3a_parts(N);
   const int part = blockIdx.x;
   const long long ci = blockIdx.y;

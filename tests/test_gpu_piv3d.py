@@ -205,3 +205,22 @@ def test_piv3d_direct_masked(gpu):
     assert worst <= MASK_PLANE_RTOL, worst
     bad = (np.abs(VF - VFo) > VF_ATOL).any(axis=0) & ~near_tie & ~sparse
     assert not bad.any(), np.abs(VF - VFo).max()
+
+
+@pytest.mark.parametrize("cfg", [((48, 40, 100), (16, 16, 16), (8, 8, 8), (8, 8, 12)),
+                                 ((40, 36, 96), (32, 32, 32), (16, 16, 16), (16, 16, 16)),
+                                 ((100, 104, 128), (32, 32, 32), (32, 32, 32), (48, 48, 32))],
+                         ids=["n32", "n64", "n128"])
+def test_host_pipeline_3d_matches_device(cfg, gpu):
+    """3D FFTCC from host arrays with at least 64 z-planes takes the pipelined
+    copy path (z-plane pieces, IA layers as their planes arrive); VF and SN
+    equal the device-array path's bit for bit."""
+    import torch
+    shape, IS, SM, st = cfg
+    i1, i2, _ = synth.pair_3d_shear(shape=shape, seed_stream=41, shift=(1.4, -0.6, 2.2))
+    pp = _params("fft", IS, SM, st)
+    VF, SN = PIV(i1, i2, pp)
+    dev = torch.device("cuda", 0)
+    VFd, SNd = PIV(torch.from_numpy(i1).to(dev), torch.from_numpy(i2).to(dev), pp)
+    assert np.array_equal(VF, VFd.cpu().numpy(), equal_nan=True)
+    assert np.array_equal(SN, SNd.cpu().numpy(), equal_nan=True)
