@@ -97,10 +97,11 @@ __global__ void k3a_merge_kernel(Piv3dArgs a, long long n) {
   a.state[ci] = s;
 }
 
-// One block of N threads per (k3, IA) slab.
+// One block of 2N threads (a pair per line) per (k3, IA) slab.
 template <int N, bool FPRUNE>
-__global__ void __launch_bounds__(N) k3b_kernel(Piv3dArgs a, float2* C) {
+__global__ void __launch_bounds__(2 * N) k3b_kernel(Piv3dArgs a, float2* C) {
   using L = Lay3<N, FPRUNE>;
+  constexpr int M = N / 2;
   extern __shared__ float2 sm[];
   const int k3 = blockIdx.x;
   const long long ci = blockIdx.y;
@@ -109,15 +110,38 @@ __global__ void __launch_bounds__(N) k3b_kernel(Piv3dArgs a, float2* C) {
   const int P1 = 2 * a.SM[0] + 1, P2 = 2 * a.SM[1] + 1;
   float2* S = sm;
   float2* SF = sm + N * L::SSTR;
-  const int t = threadIdx.x;
-  k3b_rows<N, FPRUNE>(a, g, ci, k3, t, S, SF);
+  const int t = threadIdx.x % N, h = threadIdx.x / N;
+  k3b_rows<N, FPRUNE>(a, g, ci, k3, t, h, S, SF);
   __syncthreads();
-  float2 p[N];
-  k3b_cols<N, FPRUNE>(t, S, SF, p);
+  {
+    float2 y[M];
+    k3b_cols_g<N, FPRUNE>(t, h, S, y);
+    __syncthreads();
+    k3b_park<N, FPRUNE>(t, h, S, y);
+  }
   __syncthreads();
-  k3b_store_cols<N, FPRUNE>(t, P1, p, S);
+  {
+    float2 p[M];
+    k3b_cols_f<N, FPRUNE>(t, h, S, SF, p);
+    __syncthreads();
+    k3b_x1<N, FPRUNE>(t, h, p, S);
+  }
   __syncthreads();
-  k3b_rows2<N, FPRUNE>(ci, k3, t, P1, P2, S, C);
+  {
+    float2 o[M];
+    k3b_x2<N, FPRUNE>(t, h, S, o);
+    __syncthreads();
+    k3b_x3<N, FPRUNE>(t, h, P1, o, S);
+  }
+  __syncthreads();
+  {
+    float2 u[M];
+    k3b_r2a<N, FPRUNE>(t, h, P1, S, u);
+    __syncthreads();
+    k3b_r2b<N, FPRUNE>(t, h, P1, u, S);
+  }
+  __syncthreads();
+  k3b_r2c<N, FPRUNE>(ci, k3, t, h, P1, P2, S, C);
 }
 
 // Blocks (part, IA): each part walks its contiguous share of the lag pairs;
@@ -227,7 +251,7 @@ cudaError_t run_chunks(Piv3dArgs a, long long chunk, cudaStream_t s, std::string
     for (int pass = 0; pass < NPASS; ++pass) {
       k3a_kernel<N, FPRUNE, ALG, T><<<dim3(k3a_parts(N), (unsigned)n), K3A_THREADS, 0, s>>>(a, pass);
       if (pass == 0) k3a_merge_kernel<N, ALG><<<merge_blocks, 128, 0, s>>>(a, n);
-      k3b_kernel<N, FPRUNE><<<dim3(L::K3, (unsigned)n), N, smem, s>>>(a, pass == 0 ? a.C : a.C2);
+      k3b_kernel<N, FPRUNE><<<dim3(L::K3, (unsigned)n), 2 * N, smem, s>>>(a, pass == 0 ? a.C : a.C2);
     }
     const int cparts = k3c_parts(N, (2 * a.SM[0] + 1) * (2 * a.SM[1] + 1));
     k3c_kernel<N, ALG><<<dim3(cparts, (unsigned)n), K3C_THREADS, 0, s>>>(a);

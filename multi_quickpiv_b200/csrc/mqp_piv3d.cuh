@@ -279,90 +279,178 @@ MQP_HD MQP_FI bool skip_test3(const Piv3dArgs& a, int alg, double vmax, double m
 }
 
 // ---------------------------------------------------------------------------
-// K3b: the complex 2D correlation of one k3 slab (thread t of N)
+// K3b: the complex 2D correlation of one k3 slab, two threads per line
 // ---------------------------------------------------------------------------
-// Rows: thread t transforms row x1 = t of the G slab and (t < NF) of the F
-// slab along dim 2; spectra go to S[k2][x1] and SF[k2][x1].
+// Thread (t, h) of 2N: every N-point line transform is split between a pair.
+// Forward (decimation in frequency): X[2m + h] is the M-point FFT (M = N/2)
+// of x[n] + x[n+M] (h = 0) or (x[n] - x[n+M]) W_N^n (h = 1).  Inverse
+// (decimation in time): z_h = M-point inverse of the bins of parity h, and
+// x[n] = z_0[n] + W_N^-n z_1[n], x[n+M] = z_0[n] - W_N^-n z_1[n].  A thread
+// holds M values, half the registers of a whole line, so twice the warps fit.
+// Phases are separated by block barriers (the kernel, or the host emulation
+// running each phase for all threads before the next).
+
+// the half-line input of the forward split from the line's two halves
+template <int N>
+MQP_HD MQP_FI float2 dif_in(int h, int n, float2 u, float2 v) {
+  return h ? rotate<N, false>(csub(u, v), n) : cadd(u, v);
+}
+
+// Phase R: thread (t, h) transforms row x1 = t of the G slab and (t < NF) of
+// the F slab along dim 2; bins k2 = 2m + h go to S[k2][x1] and SF[k2][x1].
 template <int N, bool FPRUNE>
-MQP_HD MQP_FI void k3b_rows(const Piv3dArgs& a, const IAGeom3& g, long long ci, int k3, int t, float2* S,
+MQP_HD MQP_FI void k3b_rows(const Piv3dArgs& a, const IAGeom3& g, long long ci, int k3, int t, int h, float2* S,
                             float2* SF) {
   using L = Lay3<N, FPRUNE>;
+  constexpr int M = N / 2;
+  const float2 z0 = make_float2(0.f, 0.f);
   if (t >= g.lo[0] && t < g.hi[0]) {
     const float2* src = a.Gz + ci * L::GZ + (long long)k3 * N * N + t;
-    float2 v[N];
+    float2 y[M];
 #pragma unroll
-    for (int x2 = 0; x2 < N; ++x2) v[x2] = (x2 >= g.lo[1] && x2 < g.hi[1]) ? src[x2 * N] : make_float2(0.f, 0.f);
-    fft_reg<N, false>(v);
+    for (int n = 0; n < M; ++n) {
+      const float2 u = (n >= g.lo[1] && n < g.hi[1]) ? src[n * N] : z0;
+      const float2 v = (n + M >= g.lo[1] && n + M < g.hi[1]) ? src[(n + M) * N] : z0;
+      y[n] = dif_in<N>(h, n, u, v);
+    }
+    fft_reg<M, false>(y);
 #pragma unroll
-    for (int k2 = 0; k2 < N; ++k2) S[k2 * L::SSTR + t] = v[fpos<N>(k2)];
+    for (int m = 0; m < M; ++m) S[(2 * m + h) * L::SSTR + t] = y[fpos<M>(m)];
   } else {
 #pragma unroll 4
-    for (int k2 = 0; k2 < N; ++k2) S[k2 * L::SSTR + t] = make_float2(0.f, 0.f);
+    for (int m = 0; m < M; ++m) S[(2 * m + h) * L::SSTR + t] = z0;
   }
   if (t < L::NF) {
     if (t < a.IS[0]) {
       const float2* src = a.Fz + ci * L::FZ + (long long)k3 * L::NF * L::NF + t;
-      float2 v[N];
+      float2 y[M];
 #pragma unroll
-      for (int x2 = 0; x2 < N; ++x2) v[x2] = (x2 < L::NF && x2 < a.IS[1]) ? src[x2 * L::NF] : make_float2(0.f, 0.f);
-      fft_reg<N, false, FPRUNE ? N / 2 : N>(v);
+      for (int n = 0; n < M; ++n) {
+        const float2 u = (n < L::NF && n < a.IS[1]) ? src[n * L::NF] : z0;
+        const float2 v = (n + M < L::NF && n + M < a.IS[1]) ? src[(n + M) * L::NF] : z0;
+        y[n] = dif_in<N>(h, n, u, v);
+      }
+      fft_reg<M, false>(y);
 #pragma unroll
-      for (int k2 = 0; k2 < N; ++k2) SF[k2 * L::FSTR + t] = v[fpos<N>(k2)];
+      for (int m = 0; m < M; ++m) SF[(2 * m + h) * L::FSTR + t] = y[fpos<M>(m)];
     } else {
 #pragma unroll 4
-      for (int k2 = 0; k2 < N; ++k2) SF[k2 * L::FSTR + t] = make_float2(0.f, 0.f);
+      for (int m = 0; m < M; ++m) SF[(2 * m + h) * L::FSTR + t] = z0;
     }
   }
 }
 
-// Columns: thread t = k2 transforms column k2 of G and of F along dim 1,
-// forms conj(F)*G and transforms it back along k1; p[fpos(s1)] = lag s1.
-// The G column is parked back in its own row of S (natural order) so only
-// one transform is live in registers at a time.
+// Phase C1: thread (t, h) transforms column k2 = t of G along dim 1 (row t
+// of S holds x1 = 0..N-1); the bins of parity h are kept in y (fpos slots).
 template <int N, bool FPRUNE>
-MQP_HD MQP_FI void k3b_cols(int t, float2* S, const float2* SF, float2 (&p)[N]) {
+MQP_HD MQP_FI void k3b_cols_g(int t, int h, const float2* S, float2 (&y)[N / 2]) {
   using L = Lay3<N, FPRUNE>;
-  float2* Srow = S + t * L::SSTR;
-  {
-    float2 v[N];
+  constexpr int M = N / 2;
+  const float2* row = S + t * L::SSTR;
 #pragma unroll
-    for (int x1 = 0; x1 < N; ++x1) v[x1] = Srow[x1];
-    fft_reg<N, false>(v);
+  for (int n = 0; n < M; ++n) y[n] = dif_in<N>(h, n, row[n], row[n + M]);
+  fft_reg<M, false>(y);
+}
+
+// Phase C2 (after a barrier): the G bins parked in their own row of S,
+// natural bin order k1, so the F transform has the registers to itself.
+template <int N, bool FPRUNE>
+MQP_HD MQP_FI void k3b_park(int t, int h, float2* S, const float2 (&y)[N / 2]) {
+  using L = Lay3<N, FPRUNE>;
+  constexpr int M = N / 2;
 #pragma unroll
-    for (int k1 = 0; k1 < N; ++k1) Srow[k1] = v[fpos<N>(k1)];
+  for (int m = 0; m < M; ++m) S[t * L::SSTR + 2 * m + h] = y[fpos<M>(m)];
+}
+
+// Phase C3: column t of F along dim 1, conj(F) G over the bins of parity h,
+// and its M-point inverse: z_h (fpos slots) of the lags along dim 1.
+template <int N, bool FPRUNE>
+MQP_HD MQP_FI void k3b_cols_f(int t, int h, const float2* S, const float2* SF, float2 (&p)[N / 2]) {
+  using L = Lay3<N, FPRUNE>;
+  constexpr int M = N / 2;
+  const float2 z0 = make_float2(0.f, 0.f);
+  const float2* frow = SF + t * L::FSTR;
+  float2 y[M];
+#pragma unroll
+  for (int n = 0; n < M; ++n) y[n] = dif_in<N>(h, n, n < L::NF ? frow[n] : z0, n + M < L::NF ? frow[n + M] : z0);
+  fft_reg<M, false>(y);
+  const float2* grow = S + t * L::SSTR;
+#pragma unroll
+  for (int m = 0; m < M; ++m) p[m] = cmulc(y[fpos<M>(m)], grow[2 * m + h]);
+  fft_reg<M, true>(p);
+}
+
+// Exchange of a pair's inverse halves through column t of T (T aliases S):
+// X1 writes z_0[n] (h = 0) or W_N^-n z_1[n] (h = 1) to row n + hM; X2 (after a
+// barrier) reads both and keeps x[n + hM] = z_0[n] +- W_N^-n z_1[n]; X3 (after
+// a barrier) stores the lags s1 < P1 to T[s1][t].
+template <int N, bool FPRUNE>
+MQP_HD MQP_FI void k3b_x1(int t, int h, const float2 (&p)[N / 2], float2* T) {
+  using L = Lay3<N, FPRUNE>;
+  constexpr int M = N / 2;
+#pragma unroll
+  for (int n = 0; n < M; ++n) {
+    const float2 w = p[fpos<M>(n)];
+    T[(n + h * M) * L::SSTR + t] = h ? rotate<N, true>(w, n) : w;
   }
-  float2 w[N];
+}
+template <int N, bool FPRUNE>
+MQP_HD MQP_FI void k3b_x2(int t, int h, const float2* T, float2 (&o)[N / 2]) {
+  using L = Lay3<N, FPRUNE>;
+  constexpr int M = N / 2;
 #pragma unroll
-  for (int x1 = 0; x1 < N; ++x1) w[x1] = x1 < L::NF ? SF[t * L::FSTR + x1] : make_float2(0.f, 0.f);
-  fft_reg<N, false, FPRUNE ? N / 2 : N>(w);
+  for (int n = 0; n < M; ++n) {
+    const float2 a = T[n * L::SSTR + t], b = T[(n + M) * L::SSTR + t];
+    o[n] = h ? csub(a, b) : cadd(a, b);
+  }
+}
+template <int N, bool FPRUNE>
+MQP_HD MQP_FI void k3b_x3(int t, int h, int P1, const float2 (&o)[N / 2], float2* T) {
+  using L = Lay3<N, FPRUNE>;
+  constexpr int M = N / 2;
 #pragma unroll
-  for (int k1 = 0; k1 < N; ++k1) p[k1] = cmulc(w[fpos<N>(k1)], Srow[k1]);
-  fft_reg<N, true>(p);
+  for (int n = 0; n < M; ++n)
+    if (n + h * M < P1) T[(n + h * M) * L::SSTR + t] = o[n];
 }
 
-// after every thread finished k3b_cols: lags s1 < P1 of column t into T[s1][t]
+// Phase R2a: thread (s1 = t < P1, h) takes the bins k2 of parity h of lag row
+// s1 and inverts them (M points); R2b (after a barrier) writes its half to
+// the row; R2c (after a barrier) combines the halves into lags s2 = n + hM
+// and stores those below P2 to C[ci][k3][s2][s1].
 template <int N, bool FPRUNE>
-MQP_HD MQP_FI void k3b_store_cols(int t, int P1, const float2 (&p)[N], float2* T) {
+MQP_HD MQP_FI void k3b_r2a(int t, int h, int P1, const float2* T, float2 (&u)[N / 2]) {
   using L = Lay3<N, FPRUNE>;
-#pragma unroll
-  for (int s1 = 0; s1 < N; ++s1)
-    if (s1 < P1) T[s1 * L::SSTR + t] = p[fpos<N>(s1)];
-}
-
-// Rows again: thread t = s1 < P1 transforms lag row s1 back along k2 and
-// writes lags s2 < P2 to C[ci][k3][s2][s1].
-template <int N, bool FPRUNE>
-MQP_HD MQP_FI void k3b_rows2(long long ci, int k3, int t, int P1, int P2, const float2* T, float2* C) {
-  using L = Lay3<N, FPRUNE>;
+  constexpr int M = N / 2;
   if (t >= P1) return;
-  float2 u[N];
 #pragma unroll
-  for (int k2 = 0; k2 < N; ++k2) u[k2] = T[t * L::SSTR + k2];
-  fft_reg<N, true>(u);
+  for (int m = 0; m < M; ++m) u[m] = T[t * L::SSTR + 2 * m + h];
+  fft_reg<M, true>(u);
+}
+template <int N, bool FPRUNE>
+MQP_HD MQP_FI void k3b_r2b(int t, int h, int P1, const float2 (&u)[N / 2], float2* T) {
+  using L = Lay3<N, FPRUNE>;
+  constexpr int M = N / 2;
+  if (t >= P1) return;
+#pragma unroll
+  for (int n = 0; n < M; ++n) {
+    const float2 w = u[fpos<M>(n)];
+    T[t * L::SSTR + n + h * M] = h ? rotate<N, true>(w, n) : w;
+  }
+}
+template <int N, bool FPRUNE>
+MQP_HD MQP_FI void k3b_r2c(long long ci, int k3, int t, int h, int P1, int P2, const float2* T, float2* C) {
+  using L = Lay3<N, FPRUNE>;
+  constexpr int M = N / 2;
+  if (t >= P1) return;
   float2* dst = C + ((ci * L::K3 + k3) * P2) * (long long)P1 + t;
 #pragma unroll
-  for (int s2 = 0; s2 < N; ++s2)
-    if (s2 < P2) dst[(long long)s2 * P1] = u[fpos<N>(s2)];
+  for (int n = 0; n < M; ++n) {
+    const int s2 = n + h * M;
+    if (s2 < P2) {
+      const float2 a = T[t * L::SSTR + n], b = T[t * L::SSTR + n + M];
+      dst[(long long)s2 * P1] = h ? csub(a, b) : cadd(a, b);
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------

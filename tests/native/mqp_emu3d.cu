@@ -77,21 +77,34 @@ static void emu3_run(Piv3dArgs a) {
     for (long long ci = 0; ci < n; ++ci) {
       if (st[ci].skip) continue;
       const IAGeom3 g = ia_geom3(a, a.ia_begin + ci);
+      // the kernel's phases, each for all 2N threads (t, h) before the next
+      // (its block barriers); a thread's M registers live in pbuf between phases
+      constexpr int M = N / 2;
+      using Reg = float2[M];
+      Reg* R = reinterpret_cast<Reg*>(pbuf.data());
       for (int k3 = 0; k3 < L::K3; ++k3) {
         float2* S = sm.data();
         float2* SF = S + N * L::SSTR;
-        for (int t = 0; t < N; ++t) k3b_rows<N, FPRUNE>(a, g, ci, k3, t, S, SF);
-        for (int t = 0; t < N; ++t) {
-          float2 p[N];
-          k3b_cols<N, FPRUNE>(t, S, SF, p);
-          memcpy(&pbuf[(size_t)t * N], p, sizeof(p));
-        }
-        for (int t = 0; t < N; ++t) {
-          float2 p[N];
-          memcpy(p, &pbuf[(size_t)t * N], sizeof(p));
-          k3b_store_cols<N, FPRUNE>(t, P1, p, S);
-        }
-        for (int t = 0; t < N; ++t) k3b_rows2<N, FPRUNE>(ci, k3, t, P1, P2, S, Cout);
+        for (int h = 0; h < 2; ++h)
+          for (int t = 0; t < N; ++t) k3b_rows<N, FPRUNE>(a, g, ci, k3, t, h, S, SF);
+        for (int h = 0; h < 2; ++h)
+          for (int t = 0; t < N; ++t) k3b_cols_g<N, FPRUNE>(t, h, S, R[h * N + t]);
+        for (int h = 0; h < 2; ++h)
+          for (int t = 0; t < N; ++t) k3b_park<N, FPRUNE>(t, h, S, R[h * N + t]);
+        for (int h = 0; h < 2; ++h)
+          for (int t = 0; t < N; ++t) k3b_cols_f<N, FPRUNE>(t, h, S, SF, R[h * N + t]);
+        for (int h = 0; h < 2; ++h)
+          for (int t = 0; t < N; ++t) k3b_x1<N, FPRUNE>(t, h, R[h * N + t], S);
+        for (int h = 0; h < 2; ++h)
+          for (int t = 0; t < N; ++t) k3b_x2<N, FPRUNE>(t, h, S, R[h * N + t]);
+        for (int h = 0; h < 2; ++h)
+          for (int t = 0; t < N; ++t) k3b_x3<N, FPRUNE>(t, h, P1, R[h * N + t], S);
+        for (int h = 0; h < 2; ++h)
+          for (int t = 0; t < N; ++t) k3b_r2a<N, FPRUNE>(t, h, P1, S, R[h * N + t]);
+        for (int h = 0; h < 2; ++h)
+          for (int t = 0; t < N; ++t) k3b_r2b<N, FPRUNE>(t, h, P1, R[h * N + t], S);
+        for (int h = 0; h < 2; ++h)
+          for (int t = 0; t < N; ++t) k3b_r2c<N, FPRUNE>(ci, k3, t, h, P1, P2, S, Cout);
       }
     }
   }

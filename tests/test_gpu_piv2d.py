@@ -164,3 +164,27 @@ def test_host_pipeline_matches_device(alg, cfg, gpu):
     VFd, SNd = PIV(torch.from_numpy(i1).to(dev), torch.from_numpy(i2).to(dev), *tm, pp)
     assert np.array_equal(VF, VFd.cpu().numpy(), equal_nan=True)
     assert np.array_equal(SN, SNd.cpu().numpy(), equal_nan=True)
+
+
+def test_host_pieces_are_invisible(gpu):
+    """MQP_TUNE_HOST_PIECES changes only how the host-array path overlaps its
+    copies: 1 (copy first), 2, 3 and 16 pieces give the same VF and SN; out
+    of range values are refused."""
+    from multi_quickpiv_b200 import _lib
+    g = np.random.default_rng(62)
+    shape = (256, 1100)
+    i1 = (g.random(shape) * 100).astype(np.float32)
+    i2 = np.roll(i1, (1, 2), axis=(0, 1)) + g.normal(0, 2, shape).astype(np.float32)
+    pp = setPIVParameters(corr_alg="zncc", interSize=32, searchMargin=16, step=8, computeSN=True)
+    ctx = _lib.Context(0)
+    ref = None
+    for pieces in (1, 2, 3, 16):
+        ctx.set_host_pieces(pieces)
+        VF, SN = PIV(i1, i2, pp, context=ctx)
+        if ref is None:
+            ref = (VF, SN)
+        assert np.array_equal(VF, ref[0]) and np.array_equal(SN, ref[1], equal_nan=True)
+    for bad in (0, 17):
+        with pytest.raises(Exception):
+            ctx.set_host_pieces(bad)
+    ctx.close()
