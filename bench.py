@@ -113,6 +113,25 @@ def dist_env():
             int(os.environ.get("WORLD_SIZE", 1)))
 
 
+def max_over_ranks(x, world, device=None):
+    """The largest of every rank's x: each rank's device time (or host time)
+    of its K steps, so the job's time is the slowest replica's.  Every rank
+    must call it, in the same order (one all-reduce)."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world, units_per_rank, steps, seconds):
+    """Whole-job throughput of `world` replicas that each processed
+    units_per_rank per step for `steps` steps in `seconds` (the max over ranks)."""
+    return world * units_per_rank * steps / seconds
+
+
 class Workload:
     """One bench workload: the image pair, its parameters and its counts."""
 
@@ -260,13 +279,9 @@ def run_ours(args):
     prof = ctx.profile_read()
     ctx.profile_enable(False)
     step_ms = [a.elapsed_time(b) for a, b in ev]
-    total_ms = sum(step_ms)
-    if world > 1:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(sum(step_ms), world, dev)
     ms_per_step = total_ms / args.steps
-    value = world * n_ia * args.steps / (total_ms / 1e3)
+    value = job_rate(world, n_ia, args.steps, total_ms / 1e3)
 
     # ---- e2e through the public API from pinned host memory ----
     npx = int(np.prod(shape))
@@ -284,12 +299,8 @@ def run_ours(args):
         t0 = time.perf_counter()
         VFh, _ = mq.PIV(h1p, h2p, wl.params, context=ctx)
         e2e_t.append(time.perf_counter() - t0)
-    e2e_s = sum(e2e_t)
-    if world > 1:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = world * n_ia * e2e_steps / e2e_s
+    e2e_s = max_over_ranks(sum(e2e_t), world, dev)
+    e2e_value = job_rate(world, n_ia, e2e_steps, e2e_s)
 
     peaks, src = measured_peaks()
     fp32_peak = 148 * 128 * 2 * peaks.get("sm_max_mhz", 1965.0) * 1e6
@@ -380,6 +391,9 @@ def pass_flops(pairs):
 
 
 def run_batch(args):
+    rank, _, world = dist_env()
+    if rank != 0:  # a single-GPU workload: under a multi-rank launch rank 0 runs it alone
+        return 0
     import torch
 
     import multi_quickpiv_b200 as mq
@@ -482,6 +496,9 @@ def run_batch(args):
 # the serving workload: Poisson arrivals of 2D+t and 3D+t requests
 # ---------------------------------------------------------------------------
 def run_serve(args):
+    rank, _, world = dist_env()
+    if rank != 0:  # a single-GPU workload: under a multi-rank launch rank 0 runs it alone
+        return 0
     from multi_quickpiv_b200 import setPIVParameters, synth
     from multi_quickpiv_b200.serve import Server
     t0 = time.time()

@@ -334,6 +334,7 @@ int run_multipass(mqp_ctx* ctx, const mqp_params* p, const void* d1, const void*
 int piv_device_impl(mqp_ctx* ctx, const void* d1, const void* d2, const void* dmask, const void* dmask_skip,
                     int dtype, int ndims, const int64_t dims[3], const mqp_params* p, double* dVF,
                     double* dSN, cudaStream_t s, double* dplanes, int64_t ia_begin, int64_t ia_end) {
+  NvtxRange nv("mqp_piv_device");
   if (dtype != MQP_F32 && dtype != MQP_F64) return fail(ctx, MQP_ERR_INVALID, "dtype must be MQP_F32 or MQP_F64");
   if (!d1 || !d2 || !dVF) return fail(ctx, MQP_ERR_INVALID, "null image or VF pointer");
   const bool masked = dmask != nullptr;
@@ -572,6 +573,7 @@ static int host_roundtrip(mqp_ctx* ctx, const void* img1, const void* img2, cons
                           const void* mask_skip, int dtype, int ndims, const int64_t dims[3],
                           const mqp_params* p, double* VF, double* SN, int64_t vf_dims_out[3],
                           double* planes, int64_t ia_begin, int64_t ia_end) {
+  NvtxRange nv("mqp_piv");
   if (!ctx) return fail(nullptr, MQP_ERR_INVALID, "null context");
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device);
@@ -815,6 +817,7 @@ extern "C" {
 
 int mqp_postprocess_device(mqp_ctx* ctx, const mqp_post_params* p, const mqp_field* f, const double* d_in,
                            const uint8_t* d_mask, double* d_out, float* d_outf, uint8_t* d_mask_out, void* stream) {
+  NvtxRange nv("mqp_postprocess_device");
   if (!ctx) return fail(nullptr, MQP_ERR_INVALID, "null context");
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device);
@@ -826,6 +829,7 @@ int mqp_postprocess_device(mqp_ctx* ctx, const mqp_post_params* p, const mqp_fie
 
 int mqp_postprocess(mqp_ctx* ctx, const mqp_post_params* p, const mqp_field* f, const double* in, const uint8_t* mask,
                     double* out, float* outf, uint8_t* mask_out) {
+  NvtxRange nv("mqp_postprocess");
   if (!ctx) return fail(nullptr, MQP_ERR_INVALID, "null context");
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device);

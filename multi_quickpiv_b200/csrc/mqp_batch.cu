@@ -521,6 +521,7 @@ int mqp_batch_plan_create(mqp_ctx* ctx, const mqp_batch_item* items, int32_t n_i
 }
 
 int mqp_batch_plan_run(mqp_plan* plan, void* stream) {
+  NvtxRange nv("mqp_batch_plan_run");
   if (!plan) return fail(nullptr, MQP_ERR_INVALID, "null plan");
   mqp_ctx* ctx = plan->ctx;
   std::lock_guard<std::mutex> lk(ctx->mu);

@@ -4,6 +4,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
 #include <string.h>
 
@@ -66,6 +67,16 @@ struct mqp_ctx {
 };
 
 namespace mqp_host {
+
+// An NVTX range over an entry point's host work (what it enqueues), named
+// after the entry point, for Nsight Systems timelines and ncu NVTX filters;
+// without a tool attached the push and pop do nothing.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 struct ProfileScope {
   mqp_ctx* ctx;

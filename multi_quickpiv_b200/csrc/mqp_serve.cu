@@ -189,6 +189,7 @@ int64_t chunk3d_of(const SrvStream& st) {
 
 // Enqueue request r of stream st on slot stream s.  Returns "" or an error.
 std::string issue(mqp_server* S, SrvStream& st, SrvRequest& r, cudaStream_t s) {
+  NvtxRange nv("mqp_server_request");
   const int cur = (int)(r.k % RING), prev = (int)((r.k - 1) % RING);
   cudaError_t e;
   auto bad = [](cudaError_t e, const char* what) { return std::string(what) + ": " + cudaGetErrorString(e); };
