@@ -109,7 +109,7 @@ T* at(const mqp_plan* p, size_t off) {
   return reinterpret_cast<T*>(static_cast<char*>(p->arena.ptr) + off);
 }
 
-int integral_kernels_2d(int W) { return 2 + ((W + 63) / 64 > 1 ? 1 : 0); }
+int integral_kernels_2d(int W) { return 2 + ((W + 63) / 64 > 1 ? 1 : 0) + ((W + 63) / 64 > 32 ? 1 : 0); }
 
 int64_t chunk_for(const mqp_batch_options& o, size_t per, int64_t n_ia) {
   int64_t chunk = o.chunk3d > 0 ? o.chunk3d

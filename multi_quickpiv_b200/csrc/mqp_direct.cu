@@ -109,8 +109,9 @@ __device__ __forceinline__ void direct2d_ia(const Piv2dArgs& a, long long ia, fl
   acc.bidx = -1;
   acc.smax = -INFINITY;
   acc.ssum = 0.0;
-  for (int s1 = lane; s1 < P1; s1 += 32)
-    finish_row<ALG>(a, g, sc, s1, P1, P2, plane + s1 * P2, R, acc, MASKED ? c1 + s1 * P2 : nullptr);
+  // similarity of every lag, the lags spread over all lanes (a plane has
+  // only 2SM1+1 rows: one row per lane would leave most lanes idle)
+  for (int q = lane; q < P1 * P2; q += 32) direct2d_finish_lag<ALG>(a, g, sc, q, P1, P2, plane, c1, R, acc);
   __syncwarp();
   double best = acc.best;
   int bidx = acc.bidx;

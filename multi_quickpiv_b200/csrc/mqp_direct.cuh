@@ -95,6 +95,18 @@ MQP_HD MQP_FI void direct2d_load(const Piv2dArgs& a, const IAGeom& g, const IASc
   }
 }
 
+// Similarity of lag q = s1 P2 + s2 from its raw correlation(s), in place in
+// the plane, taken into the peak / SN accumulators (finish_one: the same
+// values finish_row gives the FFT kernels' rows).
+template <int ALG>
+MQP_HD MQP_FI void direct2d_finish_lag(const Piv2dArgs& a, const IAGeom& g, const IAScalars& sc, int q, int P1,
+                                       int P2, double* plane, const float* c1, const LagRanges& R, PeakAcc& acc) {
+  const int s1 = q / P2, s2 = q - s1 * P2;
+  const double v = finish_one<ALG>(a, g, sc, s1, s2, plane[q], ALG == ALG_MASK_NSQECC ? (double)c1[q] : 0.0);
+  plane[q] = v;
+  acc_take(acc, R, s1, s2, P1, v);
+}
+
 // Lane's lags: plane[s1 * P2 + s2] = sum_x F(x) G(x + s).
 MQP_HD MQP_FI void direct2d_lags(const Piv2dArgs& a, int lane, int nl, const float* F, const float* G, double* plane) {
   const int IS1 = a.IS1, IS2 = a.IS2, GS = (a.IS2 + 2 * a.SM2) | 1;

@@ -91,11 +91,29 @@ __global__ void integral_rows_chunk_kernel(int H, int W, double* __restrict__ ou
   totals[r + ld * k] = acc;
 }
 
-// pass 3: every chunk k > 0 adds the sum of the totals of chunks 0..k-1
-// (chunks k0 + blockIdx.y, k0 >= 1)
+// pass 3a: per row, the running sums of the chunk totals,
+// offs[k] = ((t_0 + t_1) + ...) + t_{k-1}, for chunks k in [k0, k1), k0 >= 1,
+// continuing from offs[k0 - 1] (left by the earlier chunks).  offs lives
+// tot_plane / 2 after the totals of its plane.
+__global__ void integral_rows_prefix_kernel(int H, double* __restrict__ totals, long long tot_plane, int k0, int k1) {
+  const long long ld = (long long)H + 1;
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r > H) return;
+  totals += tot_plane * blockIdx.z;
+  double* offs = totals + tot_plane / 2;
+  double off = k0 > 1 ? offs[r + ld * (k0 - 1)] : 0.0;
+  for (int k = k0; k < k1; ++k) {
+    off = (k > 1 ? off : 0.0) + totals[r + ld * (k - 1)];
+    offs[r + ld * k] = off;
+  }
+}
+
+// pass 3b: every chunk k > 0 adds the sum of the totals of chunks 0..k-1
+// (chunks k0 + blockIdx.y, k0 >= 1): read from pass 3a's running sums, or
+// (few chunks, no pass 3a) summed here in the same order.
 __global__ void integral_rows_offset_kernel(int H, int W, double* __restrict__ out,
                                             const double* __restrict__ totals, long long out_plane,
-                                            long long tot_plane, int k0) {
+                                            long long tot_plane, int k0, int prefixed) {
   const long long ld = (long long)H + 1;
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   const int k = blockIdx.y + k0;
@@ -103,7 +121,11 @@ __global__ void integral_rows_offset_kernel(int H, int W, double* __restrict__ o
   out += out_plane * blockIdx.z;
   totals += tot_plane * blockIdx.z;
   double off = 0.0;
-  for (int q = 0; q < k; ++q) off += totals[r + ld * q];
+  if (prefixed) {
+    off = totals[tot_plane / 2 + r + ld * k];
+  } else {
+    for (int q = 0; q < k; ++q) off += totals[r + ld * q];
+  }
   const int c0 = 1 + k * ICHUNK;
   const int c1 = c0 + ICHUNK <= W + 1 ? c0 + ICHUNK : W + 1;
   for (int c = c0; c < c1; ++c) out[r + ld * c] += off;
@@ -145,13 +167,21 @@ static cudaError_t integral_planes(const void* img, int dtype, int H, int W, int
   }
   const int chunks = (W + ICHUNK - 1) / ICHUNK;
   const int k0 = x0 / ICHUNK, k1 = (x1 + ICHUNK - 1) / ICHUNK;  // row chunks of this piece
-  const long long tot_plane = (long long)(H + 1) * (chunks + 1);
+  // per plane: the chunk totals, then their running sums
+  const long long tot_plane = 2LL * (H + 1) * (chunks + 1);
   const dim3 g1((H + 1 + 127) / 128, k1 - k0, planes);
   integral_rows_chunk_kernel<<<g1, 128, 0, s>>>(H, W, out, scratch, out_plane, tot_plane, k0);
   const int ko = k0 > 1 ? k0 : 1;
   if (k1 > ko) {
+    // wide images: running sums first (linear work); up to 32 chunks the
+    // offsets sum their few totals directly (one launch fewer)
+    const int prefixed = chunks > 32;
+    if (prefixed) {
+      const dim3 gp((H + 1 + 127) / 128, 1, planes);
+      integral_rows_prefix_kernel<<<gp, 128, 0, s>>>(H, scratch, tot_plane, ko, k1);
+    }
     const dim3 g2((H + 1 + 127) / 128, k1 - ko, planes);
-    integral_rows_offset_kernel<<<g2, 128, 0, s>>>(H, W, out, scratch, out_plane, tot_plane, ko);
+    integral_rows_offset_kernel<<<g2, 128, 0, s>>>(H, W, out, scratch, out_plane, tot_plane, ko, prefixed);
   }
   return cudaGetLastError();
 }
@@ -182,8 +212,8 @@ cudaError_t launch_integral3d(const void* img, int dtype, int H, int W, int D, b
   return cudaGetLastError();
 }
 
-size_t integral2d_scratch_bytes(int H, int W) {
-  return (size_t)(H + 1) * (size_t)((W + ICHUNK - 1) / ICHUNK + 1) * sizeof(double);
+size_t integral2d_scratch_bytes(int H, int W) {  // chunk totals and their running sums
+  return 2 * (size_t)(H + 1) * (size_t)((W + ICHUNK - 1) / ICHUNK + 1) * sizeof(double);
 }
 
 size_t integral3d_scratch_bytes(int H, int W, int D) {
@@ -582,11 +612,12 @@ static cudaError_t launch_batch_t(const Piv2dBatch& b, cudaStream_t s, std::stri
 
 template <int N, bool FPRUNE, typename T>
 static cudaError_t launch_batch_alg(const Piv2dBatch& b, cudaStream_t s, std::string& err) {
+  constexpr int MINB = N == 32 ? 3 : 2;  // as launch_piv2d
   switch (b.alg) {
-    case ALG_FFTCC: return launch_batch_t<N, FPRUNE, ALG_FFTCC, T, 4, 2>(b, s, err);
-    case ALG_ZNCC: return launch_batch_t<N, FPRUNE, ALG_ZNCC, T, 4, 2>(b, s, err);
-    case ALG_NSQECC: return launch_batch_t<N, FPRUNE, ALG_NSQECC, T, 4, 2>(b, s, err);
-    case ALG_MASK_NSQECC: return launch_batch_t<N, FPRUNE, ALG_MASK_NSQECC, T, 3, 2>(b, s, err);
+    case ALG_FFTCC: return launch_batch_t<N, FPRUNE, ALG_FFTCC, T, 4, MINB>(b, s, err);
+    case ALG_ZNCC: return launch_batch_t<N, FPRUNE, ALG_ZNCC, T, 4, MINB>(b, s, err);
+    case ALG_NSQECC: return launch_batch_t<N, FPRUNE, ALG_NSQECC, T, 4, MINB>(b, s, err);
+    case ALG_MASK_NSQECC: return launch_batch_t<N, FPRUNE, ALG_MASK_NSQECC, T, 3, MINB>(b, s, err);
     default: err = "unknown correlation algorithm"; return cudaErrorInvalidValue;
   }
 }
@@ -612,7 +643,8 @@ cudaError_t launch_piv2d(const Piv2dArgs& a, int alg, cudaStream_t s, std::strin
   const int N = piv2d_fft_len(SS1, SS2);
   const bool prune = (a.IS1 <= N / 2) && (a.IS2 <= N / 2);
   if (N == 64) return prune ? launch_dt<64, true, 4, 2>(a, alg, s, err) : launch_dt<64, false, 4, 2>(a, alg, s, err);
-  if (N == 32) return prune ? launch_dt<32, true, 4, 2>(a, alg, s, err) : launch_dt<32, false, 4, 2>(a, alg, s, err);
+  // length 32 needs fewer registers: three blocks per SM (12 warps) without spill
+  if (N == 32) return prune ? launch_dt<32, true, 4, 3>(a, alg, s, err) : launch_dt<32, false, 4, 3>(a, alg, s, err);
   if (N == 128) return launch_piv2d_big(a, alg, s, err);
   err = "search window larger than 128 along some axis is not supported by the 2D kernels";
   return cudaErrorInvalidValue;

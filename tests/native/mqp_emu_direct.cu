@@ -67,8 +67,7 @@ static void emu_d2_ia(const Piv2dArgs& a, long long ia, std::vector<float>& ws) 
   acc.bidx = -1;
   acc.smax = -INFINITY;
   acc.ssum = 0.0;
-  for (int s1 = 0; s1 < P1; ++s1)
-    finish_row<ALG>(a, g, sc, s1, P1, P2, plane + s1 * P2, R, acc, MASKED ? c1 + s1 * P2 : nullptr);
+  for (int q = 0; q < P1 * P2; ++q) direct2d_finish_lag<ALG>(a, g, sc, q, P1, P2, plane, c1, R, acc);
   if (a.planes) {
     double* dst = a.planes + (ia - a.ia_begin) * (long long)P1 * P2;
     for (int i = 0; i < P1 * P2; ++i) dst[i] = plane[(i % P1) * P2 + i / P1];
