@@ -126,9 +126,9 @@ __device__ __forceinline__ void direct2d_ia(const Piv2dArgs& a, long long ia, fl
     double* dst = a.planes + (ia - a.ia_begin) * (long long)P1 * P2;
     for (int i = lane; i < P1 * P2; i += 32) dst[i] = plane[(i % P1) * P2 + i / P1];
   }
+  double r1 = -1.0, r2 = -1.0;
+  if (bidx >= 0) refine2d_warp(plane, P2, a.SM1, a.SM2, g, bidx % P1, bidx / P1, best, lane, r1, r2);
   if (lane == 0) {
-    double r1 = -1.0, r2 = -1.0;
-    if (bidx >= 0) refine2d(plane, P2, a.SM1, a.SM2, g, bidx % P1, bidx / P1, best, r1, r2);
     a.VF[2 * vfo + 0] = r1 - a.SM1 + d1;
     a.VF[2 * vfo + 1] = r2 - a.SM2 + d2;
     if (a.SN) a.SN[vfo] = sn;

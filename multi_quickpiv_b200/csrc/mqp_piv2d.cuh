@@ -798,28 +798,65 @@ MQP_HD MQP_FI double finish_one(const Piv2dArgs& a, const IAGeom& g, const IASca
 
 // gaussian_refinement + gaussian_2D (src/utils/piv_ops.jl:282-319) around the
 // 0-based peak (p1, p2) of value mx; the plane is row-contiguous (element
-// (s1, s2) at s1*P2 + s2).  Returns the refined 0-based position (unchanged
-// when the peak touches the search range edge).
+// (s1, s2) at s1*P2 + s2).  refine2d_values gives the five values whose logs
+// the fit takes (peak, up, down, left, right) and the 3x3 minimum, or false
+// when the peak touches the search range edge (position unchanged);
+// refine2d_from_logs the refined 0-based position from their logs.
+MQP_HD MQP_FI bool refine2d_values(const double* plane, int P2, int SM1, int SM2, const IAGeom& g, int p1, int p2,
+                                   double mx, double (&v)[5], double& mn) {
+  // reference test in 1-based indices: peak > 1 + TLF_off and peak < 1 + 2SM - BRB_off
+  const bool inside = (p1 + 1 > 1 + g.tlf1) && (p2 + 1 > 1 + g.tlf2) &&
+                      (p1 + 1 < 1 + 2 * SM1 - g.brb1) && (p2 + 1 < 1 + 2 * SM2 - g.brb2);
+  if (!inside) return false;
+  auto at = [&](int i, int j) { return plane[i * P2 + j]; };
+  mn = at(p1 - 1, p2 - 1);
+  for (int j = -1; j <= 1; ++j)
+    for (int i = -1; i <= 1; ++i) mn = nmin(mn, at(p1 + i, p2 + j));
+  v[0] = mx;
+  v[1] = at(p1 - 1, p2);
+  v[2] = at(p1 + 1, p2);
+  v[3] = at(p1, p2 - 1);
+  v[4] = at(p1, p2 + 1);
+  return true;
+}
+
+MQP_HD MQP_FI void refine2d_from_logs(int p1, int p2, const double (&l)[5], double& r1, double& r2) {
+  r1 = p1 + (l[1] - l[2]) / (2.0 * l[1] - 4.0 * l[0] + 2.0 * l[2]);
+  r2 = p2 + (l[3] - l[4]) / (2.0 * l[3] - 4.0 * l[0] + 2.0 * l[4]);
+}
+
 MQP_HD MQP_FI void refine2d(const double* plane, int P2, int SM1, int SM2, const IAGeom& g, int p1, int p2,
                             double mx, double& r1, double& r2) {
   r1 = p1;
   r2 = p2;
-  // reference test in 1-based indices: peak > 1 + TLF_off and peak < 1 + 2SM - BRB_off
-  const bool inside = (p1 + 1 > 1 + g.tlf1) && (p2 + 1 > 1 + g.tlf2) &&
-                      (p1 + 1 < 1 + 2 * SM1 - g.brb1) && (p2 + 1 < 1 + 2 * SM2 - g.brb2);
-  if (!inside) return;
-  auto at = [&](int i, int j) { return plane[i * P2 + j]; };
-  double mn = at(p1 - 1, p2 - 1);
-  for (int j = -1; j <= 1; ++j)
-    for (int i = -1; i <= 1; ++i) mn = nmin(mn, at(p1 + i, p2 + j));
-  const double lmx = log(1.0 + mx - mn);
-  const double up = log(1.0 + at(p1 - 1, p2) - mn);
-  const double down = log(1.0 + at(p1 + 1, p2) - mn);
-  const double left = log(1.0 + at(p1, p2 - 1) - mn);
-  const double right = log(1.0 + at(p1, p2 + 1) - mn);
-  r1 = p1 + (up - down) / (2.0 * up - 4.0 * lmx + 2.0 * down);
-  r2 = p2 + (left - right) / (2.0 * left - 4.0 * lmx + 2.0 * right);
+  double v[5], mn;
+  if (!refine2d_values(plane, P2, SM1, SM2, g, p1, p2, mx, v, mn)) return;
+  double l[5];
+  for (int k = 0; k < 5; ++k) l[k] = log(1.0 + v[k] - mn);
+  refine2d_from_logs(p1, p2, l, r1, r2);
 }
+
+#if defined(__CUDACC__)
+// refine2d for a whole warp (every lane calls it with the same peak): lanes
+// 0-4 take one log each instead of lane 0 taking all five in a row; every
+// lane returns the same position, equal to refine2d's.
+__device__ __forceinline__ void refine2d_warp(const double* plane, int P2, int SM1, int SM2, const IAGeom& g, int p1,
+                                              int p2, double mx, int lane, double& r1, double& r2) {
+  r1 = p1;
+  r2 = p2;
+  double v[5], mn;
+  if (!refine2d_values(plane, P2, SM1, SM2, g, p1, p2, mx, v, mn)) return;
+  double x = v[0];
+#pragma unroll
+  for (int k = 1; k < 5; ++k)
+    if (lane == k) x = v[k];
+  const double mine = lane < 5 ? log(1.0 + x - mn) : 0.0;
+  double l[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) l[k] = __shfl_sync(0xffffffffu, mine, k);
+  refine2d_from_logs(p1, p2, l, r1, r2);
+}
+#endif
 
 // merge two (value, first index) candidates: larger value, then smaller index
 MQP_HD MQP_FI void peak_merge(double& best, int& bidx, double ob, int oi) {
