@@ -358,7 +358,14 @@ __device__ __forceinline__ void direct3d_tiled_ia(const Piv3dArgs& a, long long 
     acc_take3(acc, R, q % P1, (q / P1) % P2, q / (P1 * P2), q, v);
   }
   block_peak(acc, red, redi, tid, nw);  // its barriers also publish V
-  if (tid == 0) direct3d_final(a, g, ia, R, V, acc.best, acc.bidx, acc.smax, acc.ssum);
+  if (tid < 32) {  // warp 0: the fit's seven logs on seven lanes
+    double r[3] = {-1.0, -1.0, -1.0};
+    if (acc.bidx >= 0) {
+      const int p[3] = {acc.bidx % P1, (acc.bidx / P1) % P2, acc.bidx / (P1 * P2)};
+      refine3d_warp(V, P1, P2, a.SM, g, p, acc.best, tid, r);
+    }
+    if (tid == 0) direct3d_final(a, g, ia, R, V, acc.best, acc.bidx, acc.smax, acc.ssum, r);
+  }
   __syncthreads();
 }
 

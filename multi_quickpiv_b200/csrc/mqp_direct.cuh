@@ -305,12 +305,16 @@ MQP_HD MQP_FI double direct3d_sim(const Piv3dArgs& a, const IAGeom3& g, const IA
 }
 
 // Vector and SN of a 3D IA from the merged accumulators and its volume
-// (k3c_final's rule; the volume lives in the warp's workspace).
+// (k3c_final's rule; the volume lives in the warp's workspace).  With r
+// given (the refined peak, e.g. from refine3d_warp) the fit is not redone.
 MQP_HD MQP_FI void direct3d_final(const Piv3dArgs& a, const IAGeom3& g, long long ia, const LagRanges3& R,
-                                  const float* V, double best, int bidx, double smax, double ssum) {
+                                  const float* V, double best, int bidx, double smax, double ssum,
+                                  const double* rgiven = nullptr) {
   const int P1 = 2 * a.SM[0] + 1, P2 = 2 * a.SM[1] + 1;
   double r[3];
-  if (bidx < 0) {
+  if (rgiven) {
+    for (int d = 0; d < 3; ++d) r[d] = rgiven[d];
+  } else if (bidx < 0) {
     r[0] = r[1] = r[2] = -1.0;
   } else {
     const int p[3] = {bidx % P1, (bidx / P1) % P2, bidx / (P1 * P2)};

@@ -571,30 +571,69 @@ MQP_HD MQP_FI void k3c_pair(const Piv3dArgs& a, const IAGeom3& g, const IA3State
 // (element (s1, s2, s3) at s1 + P1 (s2 + P2 s3)).  The minimum runs over the
 // whole 3x3x3 neighbourhood.  r is unchanged when the peak touches the
 // search range edge.
-MQP_HD MQP_FI void refine3d(const float* vol, int P1, int P2, const int SM[3], const IAGeom3& g, const int p[3],
-                            double mx, double r[3]) {
+MQP_HD MQP_FI bool refine3d_values(const float* vol, int P1, int P2, const int SM[3], const IAGeom3& g,
+                                   const int p[3], double mx, double (&v)[7], double& mn) {
   bool inside = true;
 #pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    r[d] = p[d];
-    inside = inside && (p[d] + 1 > 1 + g.tlf[d]) && (p[d] + 1 < 1 + 2 * SM[d] - g.brb[d]);
-  }
-  if (!inside) return;
+  for (int d = 0; d < 3; ++d) inside = inside && (p[d] + 1 > 1 + g.tlf[d]) && (p[d] + 1 < 1 + 2 * SM[d] - g.brb[d]);
+  if (!inside) return false;
   const long long P12 = (long long)P1 * P2;
   const float* c = vol + p[0] + (long long)P1 * p[1] + P12 * p[2];
   const long long stride[3] = {1, P1, P12};
-  double mn = (double)c[-1 - P1 - P12];
+  mn = (double)c[-1 - P1 - P12];
   for (int k = -1; k <= 1; ++k)
     for (int j = -1; j <= 1; ++j)
       for (int i = -1; i <= 1; ++i) mn = nmin(mn, (double)c[i + P1 * j + P12 * k]);
-  const double lmx = log(1.0 + mx - mn);
+  v[0] = mx;
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    const double lo = log(1.0 + (double)c[-stride[d]] - mn);
-    const double hi = log(1.0 + (double)c[stride[d]] - mn);
-    r[d] = p[d] + (lo - hi) / (2.0 * lo - 4.0 * lmx + 2.0 * hi);
+    v[1 + 2 * d] = (double)c[-stride[d]];
+    v[2 + 2 * d] = (double)c[stride[d]];
+  }
+  return true;
+}
+
+// l[0] = log of the peak term, l[1 + 2d] / l[2 + 2d] of the lower / upper
+// neighbour along axis d
+MQP_HD MQP_FI void refine3d_from_logs(const int p[3], const double (&l)[7], double r[3]) {
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double lo = l[1 + 2 * d], hi = l[2 + 2 * d];
+    r[d] = p[d] + (lo - hi) / (2.0 * lo - 4.0 * l[0] + 2.0 * hi);
   }
 }
+
+MQP_HD MQP_FI void refine3d(const float* vol, int P1, int P2, const int SM[3], const IAGeom3& g, const int p[3],
+                            double mx, double r[3]) {
+#pragma unroll
+  for (int d = 0; d < 3; ++d) r[d] = p[d];
+  double v[7], mn;
+  if (!refine3d_values(vol, P1, P2, SM, g, p, mx, v, mn)) return;
+  double l[7];
+  for (int k = 0; k < 7; ++k) l[k] = log(1.0 + v[k] - mn);
+  refine3d_from_logs(p, l, r);
+}
+
+#if defined(__CUDACC__)
+// refine3d for a whole warp (every lane calls it with the same peak): lanes
+// 0-6 take one log each; every lane returns refine3d's position.
+__device__ __forceinline__ void refine3d_warp(const float* vol, int P1, int P2, const int SM[3], const IAGeom3& g,
+                                              const int p[3], double mx, int lane, double r[3]) {
+#pragma unroll
+  for (int d = 0; d < 3; ++d) r[d] = p[d];
+  double v[7], mn;
+  if (!refine3d_values(vol, P1, P2, SM, g, p, mx, v, mn)) return;
+  double x = v[0];
+#pragma unroll
+  for (int k = 1; k < 7; ++k)
+    if (lane == k) x = v[k];
+  const double mine = lane < 7 ? log(1.0 + x - mn) : 0.0;
+  double l[7];
+#pragma unroll
+  for (int k = 0; k < 7; ++k) l[k] = __shfl_sync(0xffffffffu, mine, k);
+  refine3d_from_logs(p, l, r);
+}
+#endif
 
 // The vector and SN of one IA from the merged accumulators (thread 0 of K3c).
 MQP_HD MQP_FI void k3c_final(const Piv3dArgs& a, const IAGeom3& g, long long ci, const LagRanges3& R, double best,
