@@ -48,6 +48,10 @@ struct mqp_plan {
   std::vector<std::function<int(cudaStream_t, const cudaStream_t*)>> ops;
   std::vector<cudaStream_t> lanes;
   std::vector<cudaEvent_t> ev_join;
+  // 2D lanes: the kernel variants (groups) of one pass round run side by side
+  std::vector<cudaStream_t> lanes2d;
+  std::vector<cudaEvent_t> ev_join2d;
+  cudaEvent_t ev_fork2d = nullptr;
   cudaStream_t cap = nullptr;
   cudaEvent_t ev_fork = nullptr;
   cudaGraph_t graph = nullptr;
@@ -87,6 +91,7 @@ struct ItemPlan {
 };
 
 constexpr int LANES3D = 4;
+constexpr int LANES2D = 4;
 
 // Rough arithmetic of one 3D pass (FLOPs), for balancing pairs over lanes.
 double cost3d(const Problem& pb) {
@@ -290,6 +295,16 @@ int mqp_batch_plan_create(mqp_ctx* ctx, const mqp_batch_item* items, int32_t n_i
     e = cudaStreamCreateWithFlags(&P->lanes[ln], cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&P->ev_join[ln], cudaEventDisableTiming);
   }
+  size_t max_groups = 0;
+  for (const auto& gr : groups) max_groups = std::max(max_groups, gr.size());
+  const int n_lanes2d = max_groups > 1 ? (int)std::min<size_t>(LANES2D, max_groups) : 0;
+  P->lanes2d.assign(n_lanes2d, nullptr);
+  P->ev_join2d.assign(n_lanes2d, nullptr);
+  for (int ln = 0; ln < n_lanes2d && e == cudaSuccess; ++ln) {
+    e = cudaStreamCreateWithFlags(&P->lanes2d[ln], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&P->ev_join2d[ln], cudaEventDisableTiming);
+  }
+  if (e == cudaSuccess && n_lanes2d) e = cudaEventCreateWithFlags(&P->ev_fork2d, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&P->cap, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&P->ev_fork, cudaEventDisableTiming);
   if (e != cudaSuccess) {
@@ -414,7 +429,21 @@ int mqp_batch_plan_create(mqp_ctx* ctx, const mqp_batch_item* items, int32_t n_i
         return e2 == cudaSuccess ? MQP_OK : cuda_fail(P->ctx, e2, "batch predictor");
       });
     }
+    // several kernel variants this round: fork them onto the 2D lanes and
+    // join them back before the next round's predictors read their vectors
+    const int nl2 = groups[r].size() > 1 ? std::min<int>((int)P->lanes2d.size(), (int)groups[r].size()) : 0;
+    if (nl2) {
+      P->ops.push_back([P, nl2](cudaStream_t m, const cudaStream_t*) {
+        if (cudaEventRecord(P->ev_fork2d, m) != cudaSuccess) return fail(P->ctx, MQP_ERR_CUDA, "batch fork");
+        for (int ln = 0; ln < nl2; ++ln)
+          if (cudaStreamWaitEvent(P->lanes2d[ln], P->ev_fork2d, 0) != cudaSuccess)
+            return fail(P->ctx, MQP_ERR_CUDA, "batch fork");
+        return MQP_OK;
+      });
+    }
+    int gi = 0;
     for (const Group& g : groups[r]) {
+      const int lane2 = nl2 ? gi++ % nl2 : -1;
       mqp::Piv2dBatch b;
       b.items = at<mqp::Piv2dArgs>(P, g.items_off);
       b.prefix = at<long long>(P, g.prefix_off);
@@ -430,8 +459,17 @@ int mqp_batch_plan_create(mqp_ctx* ctx, const mqp_batch_item* items, int32_t n_i
       P->launches += 1;
       P->ops.push_back([=](cudaStream_t m, const cudaStream_t*) {
         std::string err;
-        const cudaError_t e2 = mqp::launch_piv2d_batch(b, m, err);
+        const cudaError_t e2 = mqp::launch_piv2d_batch(b, lane2 >= 0 ? P->lanes2d[lane2] : m, err);
         return e2 == cudaSuccess ? MQP_OK : fail(P->ctx, MQP_ERR_CUDA, "batch 2D launch: " + err);
+      });
+    }
+    if (nl2) {
+      P->ops.push_back([P, nl2](cudaStream_t m, const cudaStream_t*) {
+        for (int ln = 0; ln < nl2; ++ln)
+          if (cudaEventRecord(P->ev_join2d[ln], P->lanes2d[ln]) != cudaSuccess ||
+              cudaStreamWaitEvent(m, P->ev_join2d[ln], 0) != cudaSuccess)
+            return fail(P->ctx, MQP_ERR_CUDA, "batch join");
+        return MQP_OK;
       });
     }
     for (int k = 0; k < n_items; ++k) {
@@ -557,6 +595,14 @@ int mqp_batch_plan_destroy(mqp_plan* plan) {
   if (plan->ev_fork) cudaEventDestroy(plan->ev_fork);
   for (cudaEvent_t ev : plan->ev_join)
     if (ev) cudaEventDestroy(ev);
+  for (cudaEvent_t ev : plan->ev_join2d)
+    if (ev) cudaEventDestroy(ev);
+  if (plan->ev_fork2d) cudaEventDestroy(plan->ev_fork2d);
+  for (cudaStream_t ln : plan->lanes2d)
+    if (ln) {
+      cudaStreamSynchronize(ln);
+      cudaStreamDestroy(ln);
+    }
   for (cudaStream_t ln : plan->lanes)
     if (ln) cudaStreamDestroy(ln);
   if (plan->cap) cudaStreamDestroy(plan->cap);
