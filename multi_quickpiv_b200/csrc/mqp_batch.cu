@@ -223,7 +223,9 @@ int mqp_batch_plan_create(mqp_ctx* ctx, const mqp_batch_item* items, int32_t n_i
       load[ln] += w.first;
     }
   }
-  const size_t isc2d_off = ar.take(isc2d);
+  // one 2D integral scratch per 2D lane (integral images of different pairs run side by side)
+  std::vector<size_t> isc2d_off(LANES2D);
+  for (int ln = 0; ln < LANES2D; ++ln) isc2d_off[ln] = isc2d ? ar.take(isc2d) : 0;
   std::vector<size_t> isc3d_off(n_lanes), scr3d_off(n_lanes);
   for (int ln = 0; ln < n_lanes; ++ln) {
     isc3d_off[ln] = ar.take(isc3d);
@@ -295,9 +297,11 @@ int mqp_batch_plan_create(mqp_ctx* ctx, const mqp_batch_item* items, int32_t n_i
     e = cudaStreamCreateWithFlags(&P->lanes[ln], cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&P->ev_join[ln], cudaEventDisableTiming);
   }
-  size_t max_groups = 0;
+  size_t max_groups = 0, n_ii2d = 0;
   for (const auto& gr : groups) max_groups = std::max(max_groups, gr.size());
-  const int n_lanes2d = max_groups > 1 ? (int)std::min<size_t>(LANES2D, max_groups) : 0;
+  for (const ItemPlan& ip : plan) n_ii2d += (ip.n_ii && ip.it.ndims == 2) ? 1 : 0;
+  const size_t want2d = std::max(max_groups, n_ii2d);
+  const int n_lanes2d = want2d > 1 ? (int)std::min<size_t>(LANES2D, want2d) : 0;
   P->lanes2d.assign(n_lanes2d, nullptr);
   P->ev_join2d.assign(n_lanes2d, nullptr);
   for (int ln = 0; ln < n_lanes2d && e == cudaSuccess; ++ln) {
@@ -375,21 +379,34 @@ int mqp_batch_plan_create(mqp_ctx* ctx, const mqp_batch_item* items, int32_t n_i
       if (cudaStreamWaitEvent(lanes[ln], P->ev_fork, 0) != cudaSuccess) return fail(P->ctx, MQP_ERR_CUDA, "batch fork");
     return MQP_OK;
   });
+  // 2D integral images: pairs spread over the 2D lanes, joined before round 0
+  const int nl2i = n_ii2d > 1 ? (int)P->lanes2d.size() : 0;
+  if (nl2i) {
+    P->ops.push_back([P, nl2i](cudaStream_t m, const cudaStream_t*) {
+      if (cudaEventRecord(P->ev_fork2d, m) != cudaSuccess) return fail(P->ctx, MQP_ERR_CUDA, "batch fork");
+      for (int ln = 0; ln < nl2i; ++ln)
+        if (cudaStreamWaitEvent(P->lanes2d[ln], P->ev_fork2d, 0) != cudaSuccess)
+          return fail(P->ctx, MQP_ERR_CUDA, "batch fork");
+      return MQP_OK;
+    });
+  }
+  int ii2d = 0;
   for (int k = 0; k < n_items; ++k) {
     const ItemPlan& ip = plan[k];
     if (!ip.n_ii) continue;
     const bool d3 = ip.it.ndims == 3;
+    const int lane2 = (!d3 && nl2i) ? ii2d++ % nl2i : -1;
     const void* i1 = ip.it.img1;
     const void* i2 = ip.it.img2;
     const int dt = ip.it.dtype, n_ii = ip.n_ii;
     const int H = (int)ip.it.dims[0], W = (int)ip.it.dims[1], D = d3 ? (int)ip.it.dims[2] : 1;
     double* ii[3] = {at<double>(P, ip.ii_off[0]), n_ii > 1 ? at<double>(P, ip.ii_off[1]) : nullptr,
                      n_ii > 2 ? at<double>(P, ip.ii_off[2]) : nullptr};
-    double* isc = at<double>(P, d3 ? isc3d_off[ip.lane] : isc2d_off);
+    double* isc = at<double>(P, d3 ? isc3d_off[ip.lane] : isc2d_off[lane2 >= 0 ? lane2 : 0]);
     const int lane = ip.lane;
     P->launches += (int64_t)n_ii * (d3 ? integral_kernels_2d(W) + 1 : integral_kernels_2d(W));
     P->ops.push_back([=](cudaStream_t m, const cudaStream_t* lanes) {
-      cudaStream_t st = d3 ? lanes[lane] : m;
+      cudaStream_t st = d3 ? lanes[lane] : (lane2 >= 0 ? P->lanes2d[lane2] : m);
       const void* src[3] = {i2, i2, i1};
       const bool sq[3] = {true, false, false};
       for (int i = 0; i < n_ii; ++i) {
@@ -397,6 +414,15 @@ int mqp_batch_plan_create(mqp_ctx* ctx, const mqp_batch_item* items, int32_t n_i
                                   : mqp::launch_integral2d(src[i], dt, H, W, sq[i], ii[i], isc, st);
         if (e2 != cudaSuccess) return cuda_fail(P->ctx, e2, "batch integral images");
       }
+      return MQP_OK;
+    });
+  }
+  if (nl2i) {
+    P->ops.push_back([P, nl2i](cudaStream_t m, const cudaStream_t*) {
+      for (int ln = 0; ln < nl2i; ++ln)
+        if (cudaEventRecord(P->ev_join2d[ln], P->lanes2d[ln]) != cudaSuccess ||
+            cudaStreamWaitEvent(m, P->ev_join2d[ln], 0) != cudaSuccess)
+          return fail(P->ctx, MQP_ERR_CUDA, "batch join");
       return MQP_OK;
     });
   }
