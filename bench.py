@@ -258,7 +258,7 @@ def run_ours(args):
         ctx.set_chunk3d(chunk3d, 0)
     elif nd == 3:
         # launch tuning (results never depend on it): IAs per 3D chunk, timed here
-        chunk3d, tuned = tune.autotune_chunk3d(ctx, step, stream, candidates=(512, 1024, 2048, 4096))
+        chunk3d, tuned = tune.autotune_chunk3d(ctx, step, stream, candidates=(1024, 2048, 4096, 8192, 16384))
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
