@@ -3,7 +3,7 @@ import numpy as np
 
 import oracle.piv_oracle as O
 
-# FP32 FFT + FP64 normalisation vs Float64 ("Precision"):
+# FP32 FFTs and planes with FP64 normalisation, against the Float64 oracle:
 PLANE_RTOL = 2e-6      # |plane - oracle| <= PLANE_RTOL * max|oracle plane| on the searched lags
 MASK_PLANE_RTOL = 5e-5 # masked NSQECC, IAs whose mask covers >= 25 %: the FP32 FFT error scales with
                        # the whole window while the masked sums scale with the covered part
