@@ -137,7 +137,9 @@ __device__ __forceinline__ void direct2d_ia(const Piv2dArgs& a, long long ia, fl
 }
 
 template <int ALG, typename T>
-__global__ void __launch_bounds__(DWARPS * 32) direct2d_kernel(Piv2dArgs a, int words) {
+// 2D direct kernels: eight blocks (32 warps) per SM for latency hiding (64
+// registers; a few bytes of spill for the normalised algorithms)
+__global__ void __launch_bounds__(DWARPS * 32, 8) direct2d_kernel(Piv2dArgs a, int words) {
   extern __shared__ float dsm[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float* ws = dsm + (size_t)warp * words;
@@ -147,7 +149,7 @@ __global__ void __launch_bounds__(DWARPS * 32) direct2d_kernel(Piv2dArgs a, int 
 }
 
 template <int ALG, typename T>
-__global__ void __launch_bounds__(DWARPS * 32)
+__global__ void __launch_bounds__(DWARPS * 32, 8)
     direct2d_batch_kernel(const Piv2dArgs* __restrict__ items, const long long* __restrict__ prefix, int n_items,
                           long long total, int words, int grab, unsigned long long* counter) {
   extern __shared__ float dsm[];
