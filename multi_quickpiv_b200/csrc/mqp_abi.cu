@@ -336,12 +336,13 @@ int piv_device_impl(mqp_ctx* ctx, const void* d1, const void* d2, const void* dm
                     double* dSN, cudaStream_t s, double* dplanes, int64_t ia_begin, int64_t ia_end) {
   NvtxRange nv("mqp_piv_device");
   if (dtype != MQP_F32 && dtype != MQP_F64) return fail(ctx, MQP_ERR_INVALID, "dtype must be MQP_F32 or MQP_F64");
-  if (!d1 || !d2 || !dVF) return fail(ctx, MQP_ERR_INVALID, "null image or VF pointer");
+  if (!d1 || !d2) return fail(ctx, MQP_ERR_INVALID, "null image pointer");
   const bool masked = dmask != nullptr;
   Problem pb;
   int rc = resolve(ctx, p, ndims, dims, masked, 1, pb);
   if (rc != MQP_OK) return rc;
-  if (pb.n_ia == 0) return MQP_OK;
+  if (pb.n_ia == 0) return MQP_OK;  // empty vector field: nothing to write (an empty VF may have no address)
+  if (!dVF) return fail(ctx, MQP_ERR_INVALID, "null VF pointer");
   if (ia_end < 0) ia_end = pb.n_ia;
   if (ia_begin < 0 || ia_begin > ia_end || ia_end > pb.n_ia) return fail(ctx, MQP_ERR_INVALID, "IA range outside the vector field");
   if (!p->computeSN) dSN = nullptr;

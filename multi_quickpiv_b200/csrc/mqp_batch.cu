@@ -149,7 +149,7 @@ int mqp_batch_plan_create(mqp_ctx* ctx, const mqp_batch_item* items, int32_t n_i
     ip.it = items[k];
     const mqp_batch_item& it = ip.it;
     const std::string who = "batch item " + std::to_string(k) + ": ";
-    if (!it.img1 || !it.img2 || !it.VF) return fail(ctx, MQP_ERR_INVALID, who + "null image or VF pointer");
+    if (!it.img1 || !it.img2) return fail(ctx, MQP_ERR_INVALID, who + "null image pointer");
     if (it.dtype != MQP_F32 && it.dtype != MQP_F64) return fail(ctx, MQP_ERR_INVALID, who + "dtype must be MQP_F32 or MQP_F64");
     const bool masked = it.mask != nullptr;
     ip.levels = (it.params.refine && it.params.multipass > 1) ? it.params.multipass : 1;
@@ -189,6 +189,8 @@ int mqp_batch_plan_create(mqp_ctx* ctx, const mqp_batch_item* items, int32_t n_i
       if (it.ndims == 2) isc2d = std::max(isc2d, mqp::integral2d_scratch_bytes((int)it.dims[0], (int)it.dims[1]));
       else isc3d = std::max(isc3d, mqp::integral3d_scratch_bytes((int)it.dims[0], (int)it.dims[1], (int)it.dims[2]));
     }
+    // an empty vector field is never written (an empty VF may have no address)
+    if (!it.VF && ip.lev[0].pb.n_ia > 0) return fail(ctx, MQP_ERR_INVALID, who + "null VF pointer");
     for (int l = 0; l < ip.levels; ++l) {
       Level& L = ip.lev[l];
       const size_t n = (size_t)std::max<int64_t>(L.pb.n_ia, 1);

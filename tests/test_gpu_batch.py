@@ -28,6 +28,7 @@ def _pairs():
         ((80, 72, 72), "fft", 16, 8, 16, 2, False),
         ((352, 320), "nsqecc", 16, 8, 16, 3, False),  # coarse pass IS 64 / SM 32: the 128-point block kernel
         ((288, 288), "zncc", 16, 8, 16, 3, True),
+        ((24, 300), "nsqecc", 32, 16, 16, 1, False),  # shorter than the window: an empty vector field
     ]):
         if len(shape) == 2:
             i1, i2, _ = synth.pair_2d_shift(shape=shape, shift=(3.3, -2.6), seed_stream=50 + k, dtype=np.float32)

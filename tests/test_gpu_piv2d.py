@@ -188,3 +188,33 @@ def test_host_pieces_are_invisible(gpu):
         with pytest.raises(Exception):
             ctx.set_host_pieces(bad)
     ctx.close()
+
+
+@pytest.mark.parametrize("shape", [(20, 100), (100, 20), (31, 31)])
+def test_image_smaller_than_window_gives_empty_field(shape, gpu):
+    """An axis shorter than interSize has no interrogation area: the vector
+    field is empty along it (get_vectorfield_size), from host and device
+    arrays, without error."""
+    import torch
+    pp = setPIVParameters(corr_alg="nsqecc", interSize=32, searchMargin=8, step=16, computeSN=True)
+    po = _oracle_params("nsqecc", (32, 32), (8, 8), (16, 16))
+    i1 = np.random.default_rng(63).random(shape).astype(np.float32)
+    VFo, SNo = O.piv_single_pass(i1, i1, po)
+    VF, SN = PIV(i1, i1, pp)
+    assert VF.shape == VFo.shape and SN.shape == SNo.shape and VF.size == 0
+    VFd, SNd = PIV(torch.from_numpy(i1).cuda(), torch.from_numpy(i1).cuda(), pp)
+    assert tuple(VFd.shape) == VFo.shape and VFd.numel() == 0
+
+
+def test_constant_images_zncc_has_no_peak(gpu):
+    """Constant windows make every ZNCC value 0/0: the reference's peak search
+    finds no maximum above 0 (first_fullovp_peak) and reports -(SM+1) with a
+    NaN SN; the GPU path gives exactly that, like the oracle."""
+    i1 = np.full((96, 80), 5.0, dtype=np.float32)
+    IS, SM, st = (16, 16), (4, 4), (16, 16)
+    po = _oracle_params("zncc", IS, SM, st)
+    VFo, SNo = O.piv_single_pass(i1, i1, po)
+    pp = setPIVParameters(corr_alg="zncc", interSize=IS, searchMargin=SM, step=st, computeSN=True)
+    VF, SN = PIV(i1, i1, pp)
+    assert np.array_equal(VF, VFo) and np.all(VF == -(SM[0] + 1))
+    assert np.all(np.isnan(SN)) and np.all(np.isnan(SNo))

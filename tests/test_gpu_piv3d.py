@@ -224,3 +224,26 @@ def test_host_pipeline_3d_matches_device(cfg, gpu):
     VFd, SNd = PIV(torch.from_numpy(i1).to(dev), torch.from_numpy(i2).to(dev), pp)
     assert np.array_equal(VF, VFd.cpu().numpy(), equal_nan=True)
     assert np.array_equal(SN, SNd.cpu().numpy(), equal_nan=True)
+
+
+def test_volume_smaller_than_window_gives_empty_field(gpu):
+    pp = _params("fft", (16, 16, 16), (8, 8, 8), (8, 8, 8))
+    i1 = np.random.default_rng(64).random((40, 10, 40)).astype(np.float32)
+    po = O.set_piv_parameters(corr_alg="fft", interSize=(16, 16, 16), searchMargin=(8, 8, 8), step=(8, 8, 8),
+                              computeSN=True)
+    po.ndims = 3
+    VFo, SNo = O.piv_single_pass(i1, i1, po)
+    VF, SN = PIV(i1, i1, pp)
+    assert VF.shape == VFo.shape and VF.size == 0
+
+
+@pytest.mark.parametrize("IS,SM", [((8, 8, 8), (4, 4, 4)), ((16, 16, 16), (8, 8, 8))], ids=["direct", "fft"])
+def test_constant_volumes_zncc_has_no_peak(IS, SM, gpu):
+    i1 = np.full((40, 40, 40), 3.0, dtype=np.float32)
+    st = IS
+    po = O.set_piv_parameters(corr_alg="zncc", interSize=IS, searchMargin=SM, step=st, computeSN=True)
+    po.ndims = 3
+    VFo, SNo = O.piv_single_pass(i1, i1, po)
+    VF, SN = PIV(i1, i1, _params("zncc", IS, SM, st))
+    assert np.array_equal(VF, VFo) and np.all(VF == -(SM[0] + 1))
+    assert np.all(np.isnan(SN)) and np.all(np.isnan(SNo))
