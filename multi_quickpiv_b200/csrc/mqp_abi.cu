@@ -742,7 +742,7 @@ int post_resolve(mqp_ctx* ctx, const mqp_post_params* p, const mqp_field* f, mqp
       break;
     case MQP_POST_STD_MASK:
       if (f->ncomp != 1) return fail(ctx, MQP_ERR_INVALID, "STD masking takes a scalar map (ncomp = 1)");
-      if (a.n < 2) return fail(ctx, MQP_ERR_INVALID, "STD masking needs at least two values");
+      if (a.n == 1) return fail(ctx, MQP_ERR_INVALID, "STD masking needs at least two values (or none)");
       a.p0 = p->threshold;
       break;
     case MQP_POST_REPLACE:
@@ -794,6 +794,7 @@ PostIO post_io(int op) {
 int post_run(mqp_ctx* ctx, mqp::PostArgs& a, const double* d_in, const uint8_t* d_mask, double* d_out,
              float* d_outf, uint8_t* d_mask_out, cudaStream_t s) {
   const PostIO io = post_io(a.op);
+  if (a.n == 0) return MQP_OK;  // empty field: nothing to compute (its arrays may have no address)
   if (!d_in) return fail(ctx, MQP_ERR_INVALID, "null input field");
   if ((io.mask && !d_mask) || ((io.out_vec || io.out_scalar) && !d_out) || (io.outf && !d_outf) ||
       (io.mask_out && !d_mask_out))
@@ -837,6 +838,7 @@ int mqp_postprocess(mqp_ctx* ctx, const mqp_post_params* p, const mqp_field* f, 
   mqp::PostArgs a;
   int rc = post_resolve(ctx, p, f, a);
   if (rc != MQP_OK) return rc;
+  if (a.n == 0) return MQP_OK;  // empty field
   if (!in) return fail(ctx, MQP_ERR_INVALID, "null input field");
   const PostIO io = post_io(a.op);
   const bool vec_in = !(a.op == MQP_POST_TH_MASK || a.op == MQP_POST_STD_MASK);

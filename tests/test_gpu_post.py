@@ -93,3 +93,16 @@ def test_divergence(kw, vf2d):
     refs = PO.multiscale_divergence([(1, 1), (2, 2), (3, 3)], VF)
     for a, b in zip(outs, refs):
         assert np.allclose(a, b, rtol=1e-10, atol=1e-12)
+
+
+def test_empty_field(gpu):
+    """A vector field with no vectors (an image shorter than the window) passes
+    through the post-processing ops as an empty result, from host and device
+    arrays."""
+    import torch
+    VF = np.zeros((2, 0, 5))
+    assert PP.magnitudes(VF).shape == (0, 5)
+    assert PP.average(2, VF).shape == (2, 0, 5)
+    assert PP.STD_filtering(1.8, VF, replaceFun=PP.medianReplace).shape == (2, 0, 5)
+    out = PP.average(2, torch.zeros((2, 0, 5), dtype=torch.float64, device="cuda"))
+    assert tuple(out.shape) == (2, 0, 5)
