@@ -555,8 +555,8 @@ static cudaError_t launch_alg(const Piv2dArgs& a, int alg, cudaStream_t s, std::
     case ALG_FFTCC: return launch_t<N, FPRUNE, ALG_FFTCC, T, WARPS, MINB>(a, s, err);
     case ALG_ZNCC: return launch_t<N, FPRUNE, ALG_ZNCC, T, WARPS, MINB>(a, s, err);
     case ALG_NSQECC: return launch_t<N, FPRUNE, ALG_NSQECC, T, WARPS, MINB>(a, s, err);
-    // 29.7 KB per warp: three warps per block keep two blocks per SM
-    case ALG_MASK_NSQECC: return launch_t<N, FPRUNE, ALG_MASK_NSQECC, T, 3, MINB>(a, s, err);
+    // length 64: 29.7 KB per warp, three warps per block keep two blocks per SM
+    case ALG_MASK_NSQECC: return launch_t<N, FPRUNE, ALG_MASK_NSQECC, T, N == 32 ? 4 : 3, MINB>(a, s, err);
     default: err = "unknown correlation algorithm"; return cudaErrorInvalidValue;
   }
 }
@@ -612,7 +612,7 @@ static cudaError_t launch_batch_alg(const Piv2dBatch& b, cudaStream_t s, std::st
     case ALG_FFTCC: return launch_batch_t<N, FPRUNE, ALG_FFTCC, T, 4, MINB>(b, s, err);
     case ALG_ZNCC: return launch_batch_t<N, FPRUNE, ALG_ZNCC, T, 4, MINB>(b, s, err);
     case ALG_NSQECC: return launch_batch_t<N, FPRUNE, ALG_NSQECC, T, 4, MINB>(b, s, err);
-    case ALG_MASK_NSQECC: return launch_batch_t<N, FPRUNE, ALG_MASK_NSQECC, T, 3, MINB>(b, s, err);
+    case ALG_MASK_NSQECC: return launch_batch_t<N, FPRUNE, ALG_MASK_NSQECC, T, N == 32 ? 4 : 3, MINB>(b, s, err);
     default: err = "unknown correlation algorithm"; return cudaErrorInvalidValue;
   }
 }
