@@ -390,10 +390,43 @@ def pass_flops(pairs):
     return total, n_ia
 
 
+def run_batch_plan_only(args):
+    """The batch plan alone (default options, no per-pair comparison, no
+    autotuning): K timed replays after W warm-up replays, for profiling."""
+    rank, _, world = dist_env()
+    if rank != 0:
+        return 0
+    import torch
+
+    from multi_quickpiv_b200.batch import BatchPlan
+    pairs = batch_pairs()
+    plan = BatchPlan(pairs)
+    s = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        plan.run()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(s)
+    for _ in range(args.steps):
+        plan.run()
+    b.record(s)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / max(args.steps, 1)
+    info = plan.info()
+    print(json.dumps({"metric": METRIC, "value": info["total_ia"] / (ms / 1e3), "unit": UNIT, "n_gpus": 1,
+                      "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+                      "config": {"workload": "batch64 plan only (default options, L2 not flushed)",
+                                 "launches_per_run": info["launches"]}}), flush=True)
+    plan.close()
+    return 0
+
+
 def run_batch(args):
     rank, _, world = dist_env()
     if rank != 0:  # a single-GPU workload: under a multi-rank launch rank 0 runs it alone
         return 0
+    if args.plan_only:
+        return run_batch_plan_only(args)
     import torch
 
     import multi_quickpiv_b200 as mq
@@ -598,6 +631,8 @@ def main(argv=None):
                          "batch64: 64 mixed pairs with 3-pass refinement (batch plans vs per-pair calls); "
                          "serve: Poisson request streams (latency p50/p99; --steps = requests)")
     ap.add_argument("--chunk3d", type=int, default=0, help="IAs per 3D chunk (0: autotuned in warm-up)")
+    ap.add_argument("--plan-only", action="store_true",
+                    help="batch64: time the plan alone (default options), e.g. for a launch list")
     args = ap.parse_args(argv)
     if args.impl == "reference":
         return run_reference(args)
