@@ -353,8 +353,21 @@ void corr2(const PlanND& pl, const std::vector<double>& a, const std::vector<dou
   for (size_t i = 0; i < n; ++i) out[i] = w.z2[i].real() * inv;
 }
 
+// diag (nullable): per IA, MQP_CPU_DIAG doubles describing the similarity block on the lags
+// first_fullovp_peak searches: [0] largest value, [1] second largest (-inf if none), [2] largest
+// magnitude, [3] compute_SN's denominator (mean of the SN region without its maximum), [4] 1 when
+// the IA was skipped.  Test infrastructure: near-tie and SN-conditioning counts.
+constexpr int MQP_CPU_DIAG = 5;
+
 void ia_piv(const Ctx& c, const PlanND& pl, int64_t ia, const void* img1, const void* img2, const void* mask,
-            const void* mskip, int dtype, double* VF, double* SN, Work& w) {
+            const void* mskip, int dtype, double* VF, double* SN, Work& w, double* diag = nullptr) {
+  if (diag) {
+    double* d = diag + MQP_CPU_DIAG * ia;
+    d[0] = d[1] = -INFINITY;
+    d[2] = 0.0;
+    d[3] = NAN;
+    d[4] = 0.0;
+  }
   const Geo g = geo(c, ia);
   const int nd = c.nd;
   const int64_t H = c.dims[0], Wd = c.dims[1];
@@ -381,6 +394,7 @@ void ia_piv(const Ctx& c, const PlanND& pl, int64_t ia, const void* img1, const 
   if (skip) {
     for (int d = 0; d < nd; ++d) VF[nd * ia + d] = 0.0;
     if (SN) SN[ia] = 0.0;
+    if (diag) diag[MQP_CPU_DIAG * ia + 4] = 1.0;
     return;
   }
   double sumF2 = 0.0;
@@ -445,6 +459,26 @@ void ia_piv(const Ctx& c, const PlanND& pl, int64_t ia, const void* img1, const 
         }
       }
   auto S = [&](int r, int q, int z) { return sim[(size_t)r + (size_t)P0 * (q + (size_t)P1 * z)]; };
+  if (diag) {
+    double t1 = -INFINITY, t2 = -INFINITY, sc = 0.0;
+    for (int z = lo[2]; z <= hi[2]; ++z)
+      for (int q = lo[1]; q <= hi[1]; ++q)
+        for (int r = lo[0]; r <= hi[0]; ++r) {
+          const double v = S(r, q, z);
+          if (!std::isfinite(v)) continue;
+          sc = fabs(v) > sc ? fabs(v) : sc;
+          if (v > t1) {
+            t2 = t1;
+            t1 = v;
+          } else if (v > t2) {
+            t2 = v;
+          }
+        }
+    double* d = diag + MQP_CPU_DIAG * ia;
+    d[0] = t1;
+    d[1] = t2;
+    d[2] = sc;
+  }
   double disp[3] = {0, 0, 0};
   if (pk[0] < 0) {
     for (int d = 0; d < nd; ++d) disp[d] = -(double)(c.SM[d] + 1);
@@ -489,15 +523,15 @@ void ia_piv(const Ctx& c, const PlanND& pl, int64_t ia, const void* img1, const 
           sum += v;
         }
     SN[ia] = mx / ((sum - mx) / (len - 1.0));
+    if (diag) diag[MQP_CPU_DIAG * ia + 3] = (sum - mx) / (len - 1.0);
   }
 }
 
 }  // namespace
 
-extern "C" __attribute__((visibility("default"))) int mqp_cpu_piv(
-    const void* img1, const void* img2, const void* mask, const void* mask_skip, int dtype, int ndims,
-    const int64_t dims[3], const mqp_params* p, double* VF, double* SN, int nthreads, int64_t ia_begin,
-    int64_t ia_end) {
+static int cpu_piv(const void* img1, const void* img2, const void* mask, const void* mask_skip, int dtype,
+                   int ndims, const int64_t dims[3], const mqp_params* p, double* VF, double* SN, int nthreads,
+                   int64_t ia_begin, int64_t ia_end, double* diag) {
   if (ndims != 2 && ndims != 3) return MQP_ERR_INVALID;
   if (!p->unpadded) return MQP_ERR_UNSUPPORTED;
   Ctx c;
@@ -537,9 +571,24 @@ extern "C" __attribute__((visibility("default"))) int mqp_cpu_piv(
 #pragma omp for schedule(dynamic, 16)
 #endif
     for (int64_t ia = ia_begin; ia < ia_end; ++ia)
-      ia_piv(c, pl, ia, img1, img2, mask, mask_skip, dtype, VF, p->computeSN ? SN : nullptr, w);
+      ia_piv(c, pl, ia, img1, img2, mask, mask_skip, dtype, VF, p->computeSN ? SN : nullptr, w, diag);
   }
   return MQP_OK;
+}
+
+extern "C" __attribute__((visibility("default"))) int mqp_cpu_piv(
+    const void* img1, const void* img2, const void* mask, const void* mask_skip, int dtype, int ndims,
+    const int64_t dims[3], const mqp_params* p, double* VF, double* SN, int nthreads, int64_t ia_begin,
+    int64_t ia_end) {
+  return cpu_piv(img1, img2, mask, mask_skip, dtype, ndims, dims, p, VF, SN, nthreads, ia_begin, ia_end, nullptr);
+}
+
+// mqp_cpu_piv plus MQP_CPU_DIAG doubles per IA into diag (indexed by the IA's linear index)
+extern "C" __attribute__((visibility("default"))) int mqp_cpu_piv_diag(
+    const void* img1, const void* img2, const void* mask, const void* mask_skip, int dtype, int ndims,
+    const int64_t dims[3], const mqp_params* p, double* VF, double* SN, int nthreads, int64_t ia_begin,
+    int64_t ia_end, double* diag) {
+  return cpu_piv(img1, img2, mask, mask_skip, dtype, ndims, dims, p, VF, SN, nthreads, ia_begin, ia_end, diag);
 }
 
 extern "C" __attribute__((visibility("default"))) int mqp_cpu_max_threads(void) {

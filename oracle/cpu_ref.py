@@ -46,9 +46,16 @@ def load():
     return _lib
 
 
-def piv(img1, img2, cparams, mask=None, mask_skip=None, nthreads=0, ia_begin=0, ia_end=-1):
+DIAG_FIELDS = ("top1", "top2", "scale", "sn_den", "skipped")
+
+
+def piv(img1, img2, cparams, mask=None, mask_skip=None, nthreads=0, ia_begin=0, ia_end=-1, diag=False):
     """Run the C++ restatement; cparams is a multi_quickpiv_b200._lib.MqpParams
-    (the same POD the C ABI takes).  Returns (VF, SN) shaped like PIV's."""
+    (the same POD the C ABI takes).  Returns (VF, SN) shaped like PIV's, plus,
+    with diag=True, a dict of per-IA arrays (vector-field shape) describing the
+    similarity block on the lags first_fullovp_peak searches: the largest and
+    second-largest values, the largest magnitude, compute_SN's denominator and
+    a skipped flag."""
     lib = load()
     a1 = np.asarray(img1)
     dt = np.float64 if a1.dtype == np.float64 else np.float32
@@ -66,13 +73,23 @@ def piv(img1, img2, cparams, mask=None, mask_skip=None, nthreads=0, ia_begin=0, 
     VF = np.zeros((N,) + tuple(vf), dtype=np.float64, order="F")
     SN = np.zeros(tuple(vf), dtype=np.float64, order="F")
     ptr = lambda x: None if x is None else x.ctypes.data_as(C.c_void_p)
-    fn = lib.mqp_cpu_piv
+    args = [ptr(f1), ptr(f2), ptr(fm), ptr(fs), C.c_int(1 if dt == np.float64 else 0), C.c_int(N), dims,
+            C.byref(cparams), ptr(VF), ptr(SN), C.c_int(nthreads), C.c_int64(ia_begin), C.c_int64(ia_end)]
+    D = None
+    if diag:
+        D = np.zeros((len(DIAG_FIELDS),) + tuple(vf), dtype=np.float64, order="F")
+        fn = lib.mqp_cpu_piv_diag
+        args.append(ptr(D))
+    else:
+        fn = lib.mqp_cpu_piv
     fn.restype = C.c_int
-    rc = fn(ptr(f1), ptr(f2), ptr(fm), ptr(fs), C.c_int(1 if dt == np.float64 else 0), C.c_int(N), dims,
-            C.byref(cparams), ptr(VF), ptr(SN), C.c_int(nthreads), C.c_int64(ia_begin), C.c_int64(ia_end))
+    rc = fn(*args)
     if rc != 0:
         raise RuntimeError(f"mqp_cpu_piv failed: {rc}")
-    return VF, (SN if cparams.computeSN else None)
+    out = (VF, (SN if cparams.computeSN else None))
+    if diag:
+        out = out + ({k: D[i] for i, k in enumerate(DIAG_FIELDS)},)
+    return out
 
 
 def threads() -> int:

@@ -468,6 +468,27 @@ def compute_SN(cmat, SM, TLF_off, BRB_off):
         return np.float64(mx) / np.float64(avg)
 
 
+def sn_kappa(cmat, SM, TLF_off, BRB_off):
+    """Condition number of compute_SN for one IA (test infrastructure, not a
+    reference function): SN = top / den over the region compute_SN reads, so
+    an absolute error e on every similarity value moves SN by at most
+    e / |top| + e / |den| relative, to first order; kappa = scale / |top| +
+    scale / |den| with scale the largest magnitude on the lags
+    first_fullovp_peak searches ([1+TLF_off, 1+2SM-BRB_off])."""
+    lo = [1 + int(o) for o in TLF_off]
+    hi = [2 * int(m) - int(o) for m, o in zip(SM, BRB_off)]
+    sub = cmat[tuple(slice(l - 1, h) for l, h in zip(lo, hi))]
+    reg = cmat[tuple(slice(l - 1, h + 1) for l, h in zip(lo, hi))]
+    if sub.size < 2 or not np.isfinite(sub).all():
+        return np.inf
+    top = float(np.max(sub))
+    den = (float(np.sum(sub)) - top) / (sub.size - 1)
+    scale = float(np.max(np.abs(reg)))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        k = scale / abs(top) + scale / abs(den)
+    return k if np.isfinite(k) else np.inf
+
+
 # --------------------------------------------------------------------------
 # one interrogation area, end to end
 # --------------------------------------------------------------------------
@@ -529,7 +550,7 @@ def fft_size(p, isize, SS):
 
 
 def piv_single_pass(img1, img2, p: OracleParams, mask=None, mask_skip=None,
-                    predictor=None, scale=1, keep_corr=False):
+                    predictor=None, scale=1, keep_corr=False, kappa_out=None):
     """One pass of PIV_CPU (src/multi_quickPIV.jl:40-96) at ``scale``.
 
     ``predictor`` (integer array (N, *vf_size), optional) shifts each search
@@ -538,6 +559,9 @@ def piv_single_pass(img1, img2, p: OracleParams, mask=None, mask_skip=None,
     the search window is the one of a virtual interrogation area moved by the
     predictor (clamped inside the image), and the reported displacement is
     predictor + measured.
+
+    ``kappa_out`` (array of the vector-field shape, optional) receives each
+    IA's SN condition number (sn_kappa); test infrastructure.
     """
     img1 = np.asarray(img1)
     img2 = np.asarray(img2)
@@ -581,6 +605,8 @@ def piv_single_pass(img1, img2, p: OracleParams, mask=None, mask_skip=None,
         VF[(slice(None),) + vfc] = disp
         if SN is not None and scale == 1:
             SN[vfc] = compute_SN(cm, SM, SR[2], SR[3])
+        if kappa_out is not None:
+            kappa_out[vfc] = sn_kappa(cm, SM, SR[2], SR[3])
         if keep_corr:
             corrs[vfc] = cm[tuple(slice(0, 2 * int(m) + 1) for m in SM)].copy()
     if keep_corr:
@@ -588,7 +614,7 @@ def piv_single_pass(img1, img2, p: OracleParams, mask=None, mask_skip=None,
     return VF, SN
 
 
-def PIV(img1, img2, p: OracleParams, mask=None, mask_skip=None, refine=False, keep_corr=False):
+def PIV(img1, img2, p: OracleParams, mask=None, mask_skip=None, refine=False, keep_corr=False, kappa_out=None):
     """PIV (src/multi_quickPIV.jl:17-29).
 
     With ``refine=False`` (the reference's behaviour) every pass of the
@@ -599,7 +625,8 @@ def PIV(img1, img2, p: OracleParams, mask=None, mask_skip=None, refine=False, ke
     N = np.asarray(img1).ndim
     p.ndims = N
     if not refine or p.multipass <= 1:
-        return piv_single_pass(img1, img2, p, mask=mask, mask_skip=mask_skip, keep_corr=keep_corr)
+        return piv_single_pass(img1, img2, p, mask=mask, mask_skip=mask_skip, keep_corr=keep_corr,
+                               kappa_out=kappa_out)
     size = np.asarray(img1).shape
     pred = None
     prev = None
@@ -608,7 +635,7 @@ def PIV(img1, img2, p: OracleParams, mask=None, mask_skip=None, refine=False, ke
         if prev is not None:
             pred = predictor_from_coarse(prev[0], prev[1], size, p, scale)
         VF, SN = piv_single_pass(img1, img2, p, mask=mask, mask_skip=mask_skip,
-                                 predictor=pred, scale=scale)
+                                 predictor=pred, scale=scale, kappa_out=kappa_out if level == 0 else None)
         prev = (VF, scale)
     return VF, SN
 

@@ -8,7 +8,7 @@ PLANE_RTOL = 2e-6      # |plane - oracle| <= PLANE_RTOL * max|oracle plane| on t
 MASK_PLANE_RTOL = 5e-5 # masked NSQECC, IAs whose mask covers >= 25 %: the FP32 FFT error scales with
                        # the whole window while the masked sums scale with the covered part
 VF_ATOL = 1e-3         # px, whenever the integer peak agrees
-SN_RTOL = 1e-4         # plus the conditioning term |SN|^2/|max| * 1e-6
+SN_RTOL = 1e-4         # relative; widened only per IA by its computed condition number (sn_ok)
 
 
 def searched_region(shape, IS, SM, st, k):
@@ -57,6 +57,40 @@ def compare_planes(planes, oracle_corr, shape, IS, SM, st, skip=None):
     return worst, near_tie
 
 
-def sn_ok(SN, SNo):
-    tol = SN_RTOL * np.abs(SNo) + SNo ** 2 * 1e-6
-    return (np.abs(SN - SNo) <= tol) | ~np.isfinite(SNo)
+def sn_condition_from(scale, top, den):
+    """Condition number of compute_SN (src/utils/piv_ops.jl:336-367),
+    SN = top / den with den the mean of the SN region without its maximum,
+    under an absolute error of at most e on every plane value: to first order
+    |dSN| / |SN| <= e / |top| + e / |den|, so with e = PLANE_RTOL * scale the
+    relative SN error is at most PLANE_RTOL * kappa,
+    kappa = scale / |top| + scale / |den|."""
+    scale = np.asarray(scale, dtype=np.float64)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        k = scale / np.abs(top) + scale / np.abs(den)
+    return np.where(np.isfinite(k), k, np.inf)
+
+
+def sn_condition(oracle_corr, shape, IS, SM, st):
+    """Per-IA kappa (sn_condition_from) from the oracle's similarity blocks
+    (keep_corr=True), on the region compute_SN reads: [TLF_off,
+    2SM - 1 - BRB_off] per axis."""
+    vf = O.get_vectorfield_size(shape, IS, st)
+    kappa = np.full(vf, np.inf)
+    for k, cm in oracle_corr.items():
+        reg = searched_region(shape, IS, SM, st, k)
+        sreg = tuple(slice(r.start, r.stop - 1) for r in reg)
+        b = cm[sreg]
+        if b.size < 2 or not np.isfinite(b).all():
+            continue
+        top = float(np.max(b))
+        den = (float(np.sum(b)) - top) / (b.size - 1)
+        kappa[k] = sn_condition_from(float(np.max(np.abs(cm[reg]))), top, den)
+    return kappa
+
+
+def sn_ok(SN, SNo, kappa=None):
+    """|SN - SNo| <= max(SN_RTOL, PLANE_RTOL * kappa) * |SNo|: 1e-4 relative,
+    except where the IA's own condition number (sn_condition) times the plane
+    tolerance is larger.  Without kappa the plain 1e-4 applies."""
+    rel = SN_RTOL if kappa is None else np.maximum(SN_RTOL, PLANE_RTOL * np.asarray(kappa))
+    return (np.abs(SN - SNo) <= rel * np.abs(SNo)) | ~np.isfinite(SNo)

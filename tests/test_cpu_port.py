@@ -65,3 +65,29 @@ def test_port_reproduces_golden(path):
     VF, SN = CR.piv(z["img1"], z["img2"], cp, mask=mask)
     tol = 1e-7 if mask is not None else 1e-9
     assert np.allclose(VF, z["VF"], rtol=0, atol=tol, equal_nan=True)
+
+
+@pytest.mark.parametrize("alg", ["fft", "zncc", "nsqecc"])
+def test_port_diagnostics_match_numpy_planes(alg):
+    """The port's per-IA diagnostics (largest and second-largest similarity on
+    the searched lags, largest magnitude, SN denominator) agree with the NumPy
+    oracle's similarity blocks; they feed the near-tie and SN-conditioning
+    counts of the full-size parity tests."""
+    from tests.helpers import searched_region
+    IS, SM, st = (32, 32), (16, 16), (16, 16)
+    i1, i2, _ = synth.pair_2d_shift(shape=(112, 100), seed_stream=34)
+    po = O.set_piv_parameters(corr_alg=alg, interSize=IS, searchMargin=SM, step=st, computeSN=True)
+    po.ndims = 2
+    _, _, Co = O.piv_single_pass(i1, i2, po, keep_corr=True)
+    _, _, D = CR.piv(i1, i2, _params(alg, IS, SM, st), diag=True)
+    for k, cm in Co.items():
+        reg = searched_region(i1.shape, IS, SM, st, k)
+        v = np.sort(cm[reg].ravel())[::-1]
+        assert abs(D["top1"][k] - v[0]) <= 1e-9 * abs(v[0])
+        assert abs(D["top2"][k] - v[1]) <= 1e-9 * abs(v[0])
+        assert abs(D["scale"][k] - np.max(np.abs(v))) <= 1e-9 * abs(v[0])
+        sreg = tuple(slice(r.start, r.stop - 1) for r in reg)
+        b = cm[sreg]
+        den = (b.sum() - b.max()) / (b.size - 1)
+        assert abs(D["sn_den"][k] - den) <= 1e-9 * np.max(np.abs(b))
+    assert (D["skipped"] == 0).all()

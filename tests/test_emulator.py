@@ -8,7 +8,7 @@ import pytest
 
 import oracle.piv_oracle as O
 from multi_quickpiv_b200 import synth
-from tests.helpers import MASK_PLANE_RTOL, PLANE_RTOL, VF_ATOL, compare_planes, mask_coverage, sn_ok
+from tests.helpers import MASK_PLANE_RTOL, PLANE_RTOL, VF_ATOL, compare_planes, mask_coverage, sn_condition, sn_ok
 from tests.native import build_emu
 
 ALG = {"fft": 0, "zncc": 1, "nsqecc": 2}
@@ -68,7 +68,7 @@ def test_emulated_kernel_matches_oracle(emu, alg, cfg, dtype):
     assert worst <= PLANE_RTOL, worst
     bad = (np.abs(VF - VFo) > VF_ATOL).any(axis=0) & ~near_tie
     assert not bad.any()
-    assert (sn_ok(SN, SNo) | near_tie).all()
+    assert (sn_ok(SN, SNo, sn_condition(Co, i1.shape, IS, SM, st)) | near_tie).all()
 
 
 def test_emulated_threshold_skip(emu):
@@ -134,7 +134,7 @@ def test_emulated_big_window_matches_oracle(emu, alg, cfg):
     assert worst <= PLANE_RTOL, worst
     bad = (np.abs(VF - VFo) > VF_ATOL).any(axis=0) & ~near_tie
     assert not bad.any(), np.abs(VF - VFo).max()
-    assert (sn_ok(SN, SNo) | near_tie).all()
+    assert (sn_ok(SN, SNo, sn_condition(Co, i1.shape, IS, SM, st)) | near_tie).all()
 
 
 def test_emulated_big_window_masked(emu):
@@ -171,7 +171,7 @@ def test_emulated_direct_small_windows(emu, alg, cfg, dtype):
     assert worst <= PLANE_RTOL, worst
     bad = (np.abs(VF - VFo) > VF_ATOL).any(axis=0) & ~near_tie
     assert not bad.any(), np.abs(VF - VFo).max()
-    assert (sn_ok(SN, SNo) | near_tie | ~np.isfinite(SNo)).all()
+    assert (sn_ok(SN, SNo, sn_condition(Co, i1.shape, IS, SM, st)) | near_tie | ~np.isfinite(SNo)).all()
 
 
 def test_emulated_direct_masked(emu):

@@ -12,7 +12,7 @@ import pytest
 
 import oracle.piv_oracle as O
 from multi_quickpiv_b200 import synth
-from tests.helpers import MASK_PLANE_RTOL, PLANE_RTOL, VF_ATOL, compare_planes, mask_coverage, sn_ok
+from tests.helpers import MASK_PLANE_RTOL, PLANE_RTOL, VF_ATOL, compare_planes, mask_coverage, sn_condition, sn_ok
 from tests.native import build_emu
 
 ALG = {"fft": 0, "zncc": 1, "nsqecc": 2}
@@ -50,7 +50,7 @@ def check_against(VF, SN, PL, VFo, SNo, corr, shape, IS, SM, st, rtol=PLANE_RTOL
     assert worst <= rtol, worst
     bad = (np.abs(VF - VFo) > VF_ATOL).any(axis=0) & ~near_tie
     assert not bad.any(), np.abs(VF - VFo).max()
-    assert (sn_ok(SN, SNo) | near_tie).all()
+    assert (sn_ok(SN, SNo, sn_condition(corr, shape, IS, SM, st)) | near_tie).all()
 
 
 @pytest.mark.parametrize("path", GOLDEN3D, ids=lambda p: os.path.basename(p)[:-4])
@@ -145,7 +145,7 @@ def test_emulated_3d_direct_small_windows(emu, alg, cfg):
     assert worst <= PLANE_RTOL, worst
     bad = (np.abs(VF - VFo) > VF_ATOL).any(axis=0) & ~near_tie
     assert not bad.any(), np.abs(VF - VFo).max()
-    assert (sn_ok(SN, SNo) | near_tie | ~np.isfinite(SNo)).all()
+    assert (sn_ok(SN, SNo, sn_condition(Co, shape, IS, SM, st)) | near_tie | ~np.isfinite(SNo)).all()
 
 
 def test_emulated_3d_direct_masked(emu):

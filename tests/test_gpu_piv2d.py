@@ -5,7 +5,7 @@ import pytest
 
 import oracle.piv_oracle as O
 from multi_quickpiv_b200 import PIV, correlation_planes, setPIVParameters, synth
-from tests.helpers import MASK_PLANE_RTOL, PLANE_RTOL, VF_ATOL, compare_planes, mask_coverage, sn_ok
+from tests.helpers import MASK_PLANE_RTOL, PLANE_RTOL, VF_ATOL, compare_planes, mask_coverage, sn_condition, sn_ok
 
 pytestmark = pytest.mark.gpu
 
@@ -26,7 +26,7 @@ def _compare(img1, img2, alg, IS, SM, st, thr=-1.0):
     assert worst <= PLANE_RTOL, worst
     bad = (np.abs(VF - VFo) > VF_ATOL).any(axis=0) & ~near_tie
     assert not bad.any(), (np.argwhere(bad)[:5], np.abs(VF - VFo).max())
-    assert (sn_ok(SN, SNo) | near_tie).all()
+    assert (sn_ok(SN, SNo, sn_condition(Co, img1.shape, IS, SM, st)) | near_tie).all()
     return VF, VFo
 
 

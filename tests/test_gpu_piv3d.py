@@ -8,10 +8,9 @@ import os
 import numpy as np
 import pytest
 
-import oracle.cpu_ref as CR
 import oracle.piv_oracle as O
 from multi_quickpiv_b200 import PIV, correlation_planes, setPIVParameters, synth
-from tests.helpers import MASK_PLANE_RTOL, PLANE_RTOL, VF_ATOL, compare_planes, mask_coverage, sn_ok
+from tests.helpers import MASK_PLANE_RTOL, PLANE_RTOL, VF_ATOL, compare_planes, mask_coverage, sn_condition, sn_ok
 
 pytestmark = pytest.mark.gpu
 
@@ -29,7 +28,7 @@ def _check(VF, SN, planes, VFo, SNo, corr, shape, IS, SM, st, rtol=PLANE_RTOL, s
     bad = (np.abs(VF - VFo) > VF_ATOL).any(axis=0) & ~near_tie
     assert not bad.any(), (np.argwhere(bad)[:5], np.abs(VF - VFo).max())
     if SN is not None:
-        assert (sn_ok(SN, SNo) | near_tie).all()
+        assert (sn_ok(SN, SNo, sn_condition(corr, shape, IS, SM, st)) | near_tie).all()
 
 
 @pytest.mark.parametrize("path", GOLDEN3D, ids=lambda p: os.path.basename(p)[:-4])
@@ -135,34 +134,6 @@ def test_piv3d_torch_device_path(gpu):
     VF, SN = PIV(i1, i2, pp)
     VFd, SNd = PIV(torch.from_numpy(i1).cuda(), torch.from_numpy(i2).cuda(), pp)
     assert np.array_equal(VFd.cpu().numpy(), VF) and np.array_equal(SNd.cpu().numpy(), SN)
-
-
-def test_shear_workload_512x512x256_fftcc(gpu):
-    """The 512x512x256 Float32 FFTCC workload (IS 32, SM 16, step 16; 14,415
-    IAs): every vector of two sampled IA ranges (the first z layer's border
-    and a block in the middle) equals the C++ Float64 restatement's, and the
-    interior recovers the imposed shift plus shear."""
-    CR.build()
-    i1, i2, (shift, shear) = synth.pair_3d_shear()
-    IS, SM, st = (32, 32, 32), (16, 16, 16), (16, 16, 16)
-    pp = _params("fft", IS, SM, st)
-    VF, SN = PIV(i1, i2, pp)
-    assert VF.shape == (3, 31, 31, 15)
-    vf = VF.shape[1:]
-    cp = pp.to_c()
-    for a, b in ((0, 200), (7000, 7200)):
-        VFc, SNc = CR.piv(i1, i2, cp, ia_begin=a, ia_end=b)
-        for ia in range(a, b):
-            k = np.unravel_index(ia, vf, order="F")
-            assert np.all(np.abs(VF[(slice(None),) + k] - VFc[(slice(None),) + k]) <= VF_ATOL), (ia, k)
-            assert abs(SN[k] - SNc[k]) <= 1e-4 * abs(SNc[k]) + SNc[k] ** 2 * 1e-6
-    # interior: u1 = 1.5 + 0.01 z at the IA centre, u2 = -0.8, u3 = 0.6
-    inner = VF[:, 2:-2, 2:-2, 2:-2]
-    zc = (np.arange(vf[2]) * 16 + 15.5)[2:-2]
-    assert np.abs(np.median(inner[1]) - shift[1]) < 0.05
-    assert np.abs(np.median(inner[2]) - shift[2]) < 0.05
-    u1 = np.median(inner[0], axis=(0, 1))
-    assert np.max(np.abs(u1 - (shift[0] + shear * zc))) < 0.1
 
 
 DIRECT_CASES = [((24, 20, 20), (4, 4, 4), (2, 2, 2), (4, 4, 4)),
