@@ -346,8 +346,13 @@ MQP_API int mqp_postprocess(mqp_ctx* ctx, const mqp_post_params* p, const mqp_fi
  *    about 1400 x 1400.  Larger images are rejected with MQP_ERR_INVALID and
  *    a message; use mqp_piv_device for them.
  *  - The first call on a device looks up the scratch array's device address
- *    (with that device current) and caches it; make that first call before
- *    any stream capture.
+ *    (with that device current); later calls look it up again unless their
+ *    stream is capturing, in which case the address cached by an earlier
+ *    call is used: make the first call on a device before any stream capture.
+ *  - One pass only: refine with multipass > 1 (the coarse-to-fine passes of
+ *    mqp_piv_device, which keep predictors between passes) returns
+ *    MQP_ERR_UNSUPPORTED; multipass < 1 returns MQP_ERR_INVALID.  An empty
+ *    vector field returns MQP_OK without touching d_VF (which may be NULL).
  *  - All calls share the one scratch array and it keeps the last call's
  *    contents (every element is rewritten before it is read, so nothing needs
  *    clearing).  Calls whose GPU work overlaps (different streams, or

@@ -39,8 +39,21 @@ static const float2 h_twiddle[TW_N] = {
 #include "mqp_twiddles.inc"
 };
 
-// (cos, sin)(2*pi*m/256)
+// (cos, sin)(2*pi*m/256) for an index that is a compile-time constant once
+// the caller is inlined and unrolled (every twiddle of the register FFTs):
+// the table is a constant expression, so each use folds to immediate
+// operands.  Read from the __constant__ table instead, the twiddles of an
+// unrolled transform were hoisted into registers ahead of use and spilled.
+// A runtime index would build the table per thread: use twiddle_rt.
 MQP_HD MQP_FI float2 twiddle_cs(int m) {
+  constexpr float2 t[TW_N] = {
+#include "mqp_twiddles.inc"
+  };
+  return t[m & (TW_N - 1)];
+}
+
+// (cos, sin)(2*pi*m/256) for a runtime index (table set-up loops)
+MQP_HD MQP_FI float2 twiddle_rt(int m) {
 #if defined(__CUDA_ARCH__)
   return c_twiddle[m & (TW_N - 1)];
 #else

@@ -64,6 +64,17 @@ struct Piv2dBatch {
 int piv2d_warp_f2(int N, bool prune, int P1, int P2, bool masked);
 cudaError_t launch_piv2d_batch(const Piv2dBatch& b, cudaStream_t s, std::string& err);
 
+// Team variant of the fused 2D kernel (mqp_piv2d_team.cu): one IA per team
+// of N threads for FFT lengths 32 and 64 with pruned F (interrogation window
+// up to N/2) and FFTCC / ZNCC / NSQECC.  piv2d_team_ok says whether a variant
+// runs on it (launch_piv2d and launch_piv2d_batch then route there);
+// piv2d_team_f2 is a team's workspace (float2 units), which piv2d_warp_f2
+// returns for those variants.
+bool piv2d_team_ok(int N, bool prune, int alg);
+int piv2d_team_f2(int N, int P1, int P2);
+cudaError_t launch_piv2d_team(const Piv2dArgs& a, int N, int alg, cudaStream_t s, std::string& err);
+cudaError_t launch_piv2d_team_batch(const Piv2dBatch& b, cudaStream_t s, std::string& err);
+
 // Small windows (direct2d_ok / direct3d_ok): spatial correlation, one warp
 // per IA (mqp_direct.cu).  Batch plans mark these groups with N = 1; their
 // Piv2dBatch::wf2 is half the per-warp word count (piv2d_direct_words).

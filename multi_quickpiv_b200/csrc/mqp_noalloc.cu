@@ -53,16 +53,21 @@ extern "C" int mqp_piv2d_noalloc(const void* d_img1, const void* d_img2, int dty
                                  const mqp_params* p, double* d_VF, double* d_SN, void* stream, char* err,
                                  int errlen) {
   if (err && errlen > 0) err[0] = '\0';
-  if (!p || !dims || !d_img1 || !d_img2 || !d_VF)
-    return report(err, errlen, MQP_ERR_INVALID, "null argument");
+  if (!p || !dims || !d_img1 || !d_img2) return report(err, errlen, MQP_ERR_INVALID, "null argument");
   if (dtype != MQP_F32 && dtype != MQP_F64) return report(err, errlen, MQP_ERR_INVALID, "dtype must be MQP_F32 or MQP_F64");
   if (!p->unpadded)
     return report(err, errlen, MQP_ERR_UNSUPPORTED,
                   "ERROR: all gaussian_displacement should be unpadded (stored unpadded must be true)");
+  if (p->multipass < 1) return report(err, errlen, MQP_ERR_INVALID, "multipass must be >= 1");
+  // the refinement passes keep predictor and coarse vector fields between
+  // passes, which this entry point has no memory for
+  if (p->refine && p->multipass > 1)
+    return report(err, errlen, MQP_ERR_UNSUPPORTED,
+                  "multi-pass refinement (refine with multipass > 1) needs per-pass buffers; use mqp_piv_device");
   if (p->corr_alg < MQP_FFTCC || p->corr_alg > MQP_NSQECC)
     return report(err, errlen, MQP_ERR_INVALID, "corr_alg must be MQP_FFTCC, MQP_ZNCC or MQP_NSQECC");
-  if (dims[0] < 1 || dims[1] < 1 || dims[0] > (1 << 28) || dims[1] > (1 << 28))
-    return report(err, errlen, MQP_ERR_INVALID, "image extents must be in [1, 2^28]");
+  if (dims[0] < 1 || dims[1] < 1 || dims[0] > (1 << 30) || dims[1] > (1 << 30))
+    return report(err, errlen, MQP_ERR_INVALID, "image extents must be in [1, 2^30]");
   const int H = (int)dims[0], W = (int)dims[1];
   int IS[2], SM[2], st[2];
   long long vf[2];
@@ -77,7 +82,8 @@ extern "C" int mqp_piv2d_noalloc(const void* d_img1, const void* d_img2, int dty
   }
   if (mqp::piv2d_fft_len(IS[0] + 2 * SM[0], IS[1] + 2 * SM[1]) == 0)
     return report(err, errlen, MQP_ERR_UNSUPPORTED, "2D search window (interSize + 2 searchMargin) above 128");
-  if (vf[0] * vf[1] == 0) return MQP_OK;
+  if (vf[0] * vf[1] == 0) return MQP_OK;  // empty vector field: nothing to write (VF may have no address)
+  if (!d_VF) return report(err, errlen, MQP_ERR_INVALID, "null VF pointer");
 
   // scratch plan: [II of img2^2 | II of img2 | II of img1 | scan totals]
   const int n_ii = p->corr_alg == MQP_NSQECC ? 1 : (p->corr_alg == MQP_ZNCC ? 3 : 0);
@@ -90,17 +96,29 @@ extern "C" int mqp_piv2d_noalloc(const void* d_img1, const void* d_img2, int dty
                       std::to_string((size_t)MQP_NOALLOC_SCRATCH_BYTES) +
                       " bytes built into mqp_piv2d_noalloc (MQP_NOALLOC_SCRATCH_BYTES); use mqp_piv_device");
 
-  // once per device, with that device current: the device address of the
-  // scratch array (the first call on a device does this; make it before any
-  // stream capture)
+  // The device address of the scratch array, with the device current.  The
+  // first call on a device looks it up; later calls look it up again unless
+  // their stream is capturing (a module reloaded after cudaDeviceReset can
+  // place the array elsewhere), and a capturing call uses the address cached
+  // by an earlier call on the device, so make one call before any capture.
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices)
     return report(err, errlen, MQP_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+  cudaStream_t s = stream ? (cudaStream_t)stream : cudaStreamLegacy;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) {
+    cudaGetLastError();  // clear the query's error; treat the stream as capturing
+    cap = cudaStreamCaptureStatusActive;
+  }
   unsigned char* base = nullptr;
   {
     std::lock_guard<std::mutex> lk(g_setup_mu);
-    if (!g_scratch_addr[dev]) {
+    if (cap == cudaStreamCaptureStatusNone || !g_scratch_addr[dev]) {
+      if (cap != cudaStreamCaptureStatusNone)
+        return report(err, errlen, MQP_ERR_INVALID,
+                      "the first call on a device must come before any stream capture (it looks up the scratch "
+                      "array's address)");
       void* ptr = nullptr;
       e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
       if (e != cudaSuccess || !ptr)
@@ -110,7 +128,6 @@ extern "C" int mqp_piv2d_noalloc(const void* d_img1, const void* d_img2, int dty
     base = static_cast<unsigned char*>(g_scratch_addr[dev]);
   }
 
-  cudaStream_t s = stream ? (cudaStream_t)stream : cudaStreamLegacy;
   double* IIg2 = n_ii >= 1 ? reinterpret_cast<double*>(base) : nullptr;
   double* IIg = n_ii >= 3 ? reinterpret_cast<double*>(base + ii_bytes) : nullptr;
   double* II1 = n_ii >= 3 ? reinterpret_cast<double*>(base + 2 * ii_bytes) : nullptr;

@@ -460,7 +460,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) piv2d_kernel(Piv2dArgs a) {
   const int wf2 = Lay::warp_f2(P1, P2, MASKED);
   float2* GH = smem + (size_t)warp * wf2;
   float2* tw = smem + (size_t)WARPS * wf2;  // (cos, sin)(2 pi j / N)
-  for (int j = threadIdx.x; j < N; j += blockDim.x) tw[j] = twiddle_cs(j * (TW_N / N));
+  for (int j = threadIdx.x; j < N; j += blockDim.x) tw[j] = twiddle_rt(j * (TW_N / N));
   __syncthreads();
   const long long nwarps = (long long)gridDim.x * WARPS;
   for (long long ia = a.ia_begin + (long long)blockIdx.x * WARPS + warp; ia < a.ia_end; ia += nwarps)
@@ -480,7 +480,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float2* GH = smem + (size_t)warp * wf2;
   float2* tw = smem + (size_t)WARPS * wf2;
-  for (int j = threadIdx.x; j < N; j += blockDim.x) tw[j] = twiddle_cs(j * (TW_N / N));
+  for (int j = threadIdx.x; j < N; j += blockDim.x) tw[j] = twiddle_rt(j * (TW_N / N));
   __syncthreads();
   for (;;) {
     unsigned long long g0 = 0;
@@ -568,6 +568,7 @@ static cudaError_t launch_dt(const Piv2dArgs& a, int alg, cudaStream_t s, std::s
 }
 
 int piv2d_warp_f2(int N, bool prune, int P1, int P2, bool masked) {
+  if (!masked && piv2d_team_ok(N, prune, ALG_NSQECC)) return piv2d_team_f2(N, P1, P2);
   if (N == 128) return piv2d_big_warp_f2(prune, P1, P2, masked);
   if (N == 64) return prune ? Layout2d<64, true>::warp_f2(P1, P2, masked) : Layout2d<64, false>::warp_f2(P1, P2, masked);
   if (N == 32) return prune ? Layout2d<32, true>::warp_f2(P1, P2, masked) : Layout2d<32, false>::warp_f2(P1, P2, masked);
@@ -626,6 +627,7 @@ cudaError_t launch_piv2d_batch(const Piv2dBatch& b, cudaStream_t s, std::string&
   if (b.total <= 0 || b.n_items <= 0) return cudaSuccess;
   if (b.N == 128) return launch_piv2d_big_batch(b, s, err);
   if (b.N == 1) return launch_piv2d_direct_batch(b, s, err);
+  if (piv2d_team_ok(b.N, b.prune, b.alg)) return launch_piv2d_team_batch(b, s, err);
   if (b.N == 64) return b.prune ? launch_batch_dt<64, true>(b, s, err) : launch_batch_dt<64, false>(b, s, err);
   if (b.N == 32) return b.prune ? launch_batch_dt<32, true>(b, s, err) : launch_batch_dt<32, false>(b, s, err);
   err = "search window larger than 64 along some axis is not supported by the 2D kernel";
@@ -637,6 +639,7 @@ cudaError_t launch_piv2d(const Piv2dArgs& a, int alg, cudaStream_t s, std::strin
   const int SS1 = a.IS1 + 2 * a.SM1, SS2 = a.IS2 + 2 * a.SM2;
   const int N = piv2d_fft_len(SS1, SS2);
   const bool prune = (a.IS1 <= N / 2) && (a.IS2 <= N / 2);
+  if (piv2d_team_ok(N, prune, alg)) return launch_piv2d_team(a, N, alg, s, err);
   if (N == 64) return prune ? launch_dt<64, true, 4, 2>(a, alg, s, err) : launch_dt<64, false, 4, 2>(a, alg, s, err);
   // length 32 needs fewer registers: three blocks per SM (12 warps) without spill
   if (N == 32) return prune ? launch_dt<32, true, 4, 3>(a, alg, s, err) : launch_dt<32, false, 4, 3>(a, alg, s, err);

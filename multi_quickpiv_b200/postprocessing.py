@@ -45,11 +45,15 @@ def _as_field(arrays):
 
 
 def _radius4(radius, nd):
+    """toDims3(radius)[1:N] (src/piv_parameters.jl:8-11, as localOp takes it,
+    postprocessing.jl:65,74,85): an Integer repeats on every axis, a shorter
+    tuple is padded with radius 0 (a 2-tuple on a 3D field averages in-plane
+    only)."""
     if np.isscalar(radius):
         r = [int(radius)] * nd
     else:
         r = [int(x) for x in radius][:nd]
-        r += [r[-1]] * (nd - len(r))
+        r += [0] * (nd - len(r))
     return (C.c_int32 * 4)(*(r + [0] * (4 - nd)))
 
 
@@ -152,7 +156,8 @@ def average_NDT(radius1, radius2, *arrays, context=None):
     VF = _as_field(arrays)
     g = _grid(VF)
     r1 = [int(radius1)] * (len(g) - 1) if np.isscalar(radius1) else [int(x) for x in radius1]
-    return average(tuple(r1[:len(g) - 1]) + (int(radius2),), VF, context=context)
+    r1 = (r1 + [0] * len(g))[:len(g) - 1]  # toDims3 padding of the spatial radii
+    return average(tuple(r1) + (int(radius2),), VF, context=context)
 
 
 def collectiveness(radius, *arrays, max_angle=40, context=None):
@@ -339,6 +344,11 @@ def divergence(radii, VF, normalize=False, min_speed=0, divide_by="N", circle=Fa
     summed over components, / count ("N") or / local |VF| sum ("mags")."""
     g = _grid(VF)
     dv = {"N": _lib.MQP_DIVIDE_N, "mags": _lib.MQP_DIVIDE_MAGS}.get(divide_by, _lib.MQP_DIVIDE_NONE)
+    # divergence uses its radii as given (normalize_sink, postprocessing.jl:757-781):
+    # a shorter tuple repeats its last entry
+    if not np.isscalar(radii):
+        r = [int(x) for x in radii][:len(g)]
+        radii = tuple(r + [r[-1]] * (len(g) - len(r)))
     p = _params(_lib.MQP_POST_DIVERGENCE, radii, len(g), normalize=int(bool(normalize)),
                 min_speed=float(min_speed), divide_by=dv, circle=int(bool(circle)))
     out, _, _ = _run(_lib.MQP_POST_DIVERGENCE, VF, VF.shape[0], g, p, out_scalar=True, context=context)

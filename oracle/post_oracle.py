@@ -27,9 +27,24 @@ def _window(idx, radius, size):
 
 
 def _radii(radius, nd):
+    """toDims3(radius)[1:N] as localOp and the window operations take it
+    (postprocessing.jl:65,74,85; toDims3, src/piv_parameters.jl:8-11): an
+    Integer repeats on every axis, a 2-tuple gets radius 0 on axis 3.  Grids
+    of 4 axes (space-time fields) take a 4-tuple as given and pad shorter
+    tuples with 0 the same way."""
     if np.isscalar(radius):
         return (int(radius),) * nd
     r = tuple(int(x) for x in radius)
+    return (r + (0,) * nd)[:nd]
+
+
+def _sink_radii(radii, nd):
+    """divergence's radii, which it uses as given (normalize_sink,
+    postprocessing.jl:757-781): an Integer repeats, a shorter tuple repeats
+    its last entry."""
+    if np.isscalar(radii):
+        return (int(radii),) * nd
+    r = tuple(int(x) for x in radii)
     return (r + (r[-1],) * nd)[:nd] if len(r) < nd else r[:nd]
 
 
@@ -278,7 +293,7 @@ def divergence(radii, VF, normalize=False, min_speed=0, divide_by="N", circle=Fa
     components of FFTCC_crop(sink_c, VFn_c), divided by the count of non-zero
     sink magnitudes ("N") or the window sum of |VFn| ("mags")."""
     VF = np.asarray(VF, dtype=np.float64)
-    radii = _radii(radii, VF.ndim - 1)
+    radii = _sink_radii(radii, VF.ndim - 1)
     VFn = normalize_vectorfield(VF, normalize=normalize, min_speed=min_speed)
     sm = normalize_sink(radii, typ=np.float64, circle=circle)
     out = np.zeros(VF.shape[1:])
@@ -303,7 +318,7 @@ def multiscale_divergence(radii_list, VF, min_value=0.2, normalize=True, min_spe
     sc = np.zeros(size, dtype=np.int64)
     for rad in radii_list:
         d = -1 * divergence(rad, VF, normalize=normalize, min_speed=min_speed, divide_by=divide_by)
-        rr = _radii(rad, len(size))[0]
+        rr = _sink_radii(rad, len(size))[0]
         for i in np.ndindex(*size):
             divg = d[i]
             conv = -1 * divg

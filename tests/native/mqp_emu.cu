@@ -5,12 +5,14 @@
 // geometry and peak logic can be checked against the oracle without a GPU.
 #include <math.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <vector>
 
 #include "mqp_direct.cuh"
 #include "mqp_piv2d.cuh"
+#include "mqp_piv2d_team.cuh"
 
 using namespace mqp;
 
@@ -39,7 +41,7 @@ static void emu_ia(const Piv2dArgs& a, long long ia, std::vector<float2>& ws) {
   double* plane = reinterpret_cast<double*>(FH);
   float* c1buf = MASKED ? reinterpret_cast<float*>(FH + Lay::region2_f2(P1, P2)) : nullptr;
   float2 tw[N];
-  for (int j = 0; j < N; ++j) tw[j] = twiddle_cs(j * (TW_N / N));
+  for (int j = 0; j < N; ++j) tw[j] = twiddle_rt(j * (TW_N / N));
   const double scale = cc_scale<N>();
   const int lane_rows = (P1 - 32 > 0 && P1 - 32 <= 4) ? 32 : P1;
   const int v1 = (int)(ia % a.vf1), v2 = (int)(ia / a.vf1);
@@ -159,6 +161,120 @@ static void emu_run(const Piv2dArgs& a) {
   }
 }
 
+// The team kernel (mqp_piv2d_team.cuh) thread by thread: each phase runs for
+// every thread of the team before the next (the team barriers), phase 2 in
+// its two halves around its barrier; the finish uses the same similarity,
+// peak and fit functions with sequential reductions.
+template <int N, int ALG, typename T>
+static void emu_team_ia(const Piv2dArgs& a, long long ia, std::vector<float2>& ws) {
+  using L = TeamLayout<N>;
+  constexpr int M = N / 2;
+  constexpr bool ZN = ALG == ALG_ZNCC;
+  const int P1 = 2 * a.SM1 + 1, P2 = 2 * a.SM2 + 1;
+  float2* G = ws.data();
+  float2* F = G + L::g_f2(P1, P2);
+  float2 tw[N];
+  for (int j = 0; j < N; ++j) tw[j] = twiddle_rt(j * (TW_N / N));
+  const int v1 = (int)(ia % a.vf1), v2 = (int)(ia / a.vf1);
+  int d1, d2;
+  ia_pred(a, v1, v2, d1, d2);
+  const IAGeom g = ia_geom(a, v1, v2);
+  IAScalars sc;
+  sc.meanF = sc.meanG = 0.0;
+  if (ZN) {
+    sc.meanF = box_sum(a.II1, a.H, g.ir1, g.ir1 + a.IS1, g.ir2, g.ir2 + a.IS2) / ((double)a.IS1 * a.IS2);
+    const double nG = (double)(g.hi1 - g.lo1) * (double)(g.hi2 - g.lo2);
+    sc.meanG = box_sum(a.IIg, a.H, g.g01 + g.lo1, g.g01 + g.hi1, g.g02 + g.lo2, g.g02 + g.hi2) / nG;
+  }
+  const long long vfo = (long long)v1 + (long long)a.vf1 * v2;
+  double vmax = -INFINITY, sumsq = 0.0;
+  for (int tid = 0; tid < N; ++tid) {
+    const int hh = tid / M, q = tid % M;
+    if (hh == 0) team_f_row<N, T, ZN, 0>(a, g, sc.meanF, q, F, vmax, sumsq);
+    else team_f_row<N, T, ZN, 1>(a, g, sc.meanF, q, F, vmax, sumsq);
+  }
+  for (int tid = 0; tid < N; ++tid) team_g_row<N, T, ZN>(a, g, (float)sc.meanG, tid, G);
+  sc.sumF2 = sumsq;
+  if (a.threshold >= 0.0 && vmax < a.threshold) {
+    a.VF[2 * vfo] = a.VF[2 * vfo + 1] = 0.0;
+    if (a.SN) a.SN[vfo] = 0.0;
+    if (a.planes)
+      for (int i = 0; i < P1 * P2; ++i) a.planes[(ia - a.ia_begin) * (long long)P1 * P2 + i] = 0.0;
+    return;
+  }
+  std::vector<float2> xs((size_t)N * M);
+  for (int tid = 0; tid < N; ++tid) {
+    float2(&x)[M] = *reinterpret_cast<float2(*)[M]>(&xs[(size_t)tid * M]);
+    if (tid / M == 0) team_p2_fold<N, 0>(tid % M, G, x);
+    else team_p2_fold<N, 1>(tid % M, G, x);
+  }
+  for (int tid = 0; tid < N; ++tid) {
+    const float2(&x)[M] = *reinterpret_cast<const float2(*)[M]>(&xs[(size_t)tid * M]);
+    if (tid / M == 0) team_p2_corr<N, 0>(tid % M, G, F, x);
+    else team_p2_corr<N, 1>(tid % M, G, F, x);
+  }
+  float* cc = reinterpret_cast<float*>(F);
+  const float scale = (float)cc_scale<N>();
+  const bool tail = P1 == M + 1;
+  const int paired = tail ? P1 - 1 : P1;
+  for (int b = 0; b < paired; b += M)
+    for (int tid = 0; tid < N; ++tid) {
+      const int s1 = b + tid % M;
+      if (s1 >= paired) continue;
+      if (tid / M == 0) team_phase3_row<N, 0>(s1, P1, P2, G, cc, scale);
+      else team_phase3_row<N, 1>(s1, P1, P2, G, cc, scale);
+    }
+  if (tail)
+    for (int s2 = 0; s2 < P2; ++s2) cc[(P1 - 1) + P1 * s2] = team_tail_value<N>(G, tw, s2) * scale;
+  double* plane = reinterpret_cast<double*>(G);
+  LagRanges R;
+  R.lo1 = g.tlf1;
+  R.hi1 = 2 * a.SM1 - g.brb1;
+  R.lo2 = g.tlf2;
+  R.hi2 = 2 * a.SM2 - g.brb2;
+  R.shi1 = 2 * a.SM1 - 1 - g.brb1;
+  R.shi2 = 2 * a.SM2 - 1 - g.brb2;
+  PeakAcc acc;
+  acc.best = 0.0;
+  acc.bidx = -1;
+  acc.smax = -INFINITY;
+  acc.ssum = 0.0;
+  const float sqF = sqrtf((float)sc.sumF2);
+  for (int l = 0; l < P1 * P2; ++l) {
+    const int s1 = l % P1, s2 = l / P1;
+    const double v = team_similarity<ALG>(a, g, sc, sqF, s1, s2, (double)cc[l]);
+    plane[s1 * P2 + s2] = v;
+    acc_take(acc, R, s1, s2, P1, v);
+    if (a.planes) a.planes[(ia - a.ia_begin) * (long long)P1 * P2 + l] = v;
+  }
+  double r1 = -1.0, r2 = -1.0;
+  if (acc.bidx >= 0) refine2d(plane, P2, a.SM1, a.SM2, g, acc.bidx % P1, acc.bidx / P1, acc.best, r1, r2);
+  a.VF[2 * vfo + 0] = r1 - a.SM1 + d1;
+  a.VF[2 * vfo + 1] = r2 - a.SM2 + d2;
+  if (a.SN) {
+    const double len = (double)(R.shi1 - R.lo1 + 1) * (double)(R.shi2 - R.lo2 + 1);
+    a.SN[vfo] = acc.smax / ((acc.ssum - acc.smax) / (len - 1.0));
+  }
+}
+
+template <int N, int ALG>
+static void emu_team_run(const Piv2dArgs& a) {
+  std::vector<float2> ws((size_t)TeamLayout<N>::team_f2(2 * a.SM1 + 1, 2 * a.SM2 + 1));
+  for (long long ia = a.ia_begin; ia < a.ia_end; ++ia) {
+    if (a.dtype == 0) emu_team_ia<N, ALG, float>(a, ia, ws);
+    else emu_team_ia<N, ALG, double>(a, ia, ws);
+  }
+}
+
+template <int N>
+static int emu_team(const Piv2dArgs& a, int alg) {
+  if (alg == 0) emu_team_run<N, 0>(a);
+  else if (alg == 1) emu_team_run<N, 1>(a);
+  else if (alg == 2) emu_team_run<N, 2>(a);
+  else return -1;
+  return 0;
+}
+
 template <int N, bool FPRUNE>
 static int emu_alg(const Piv2dArgs& a, int alg) {
   if (alg == 0) emu_run<N, FPRUNE, 0>(a);
@@ -210,8 +326,12 @@ extern "C" __attribute__((visibility("default"))) int mqp_emu_piv2d(
   const bool prune = IS1 <= N / 2 && IS2 <= N / 2;
   if (direct2d_ok(IS1, IS2, SM1, SM2)) return emu_piv2d_direct(a, alg);
   if (N == 128) return emu_piv2d_big(a, alg);
-  if (N == 64) return prune ? emu_alg<64, true>(a, alg) : emu_alg<64, false>(a, alg);
-  if (N == 32) return prune ? emu_alg<32, true>(a, alg) : emu_alg<32, false>(a, alg);
+  // as launch_piv2d: pruned FFTCC / ZNCC / NSQECC run on the team kernel
+  // (MQP_EMU_PIV2D_WARP=1 emulates the one-warp-per-IA kernel for them)
+  const char* warp_env = getenv("MQP_EMU_PIV2D_WARP");
+  const bool team = prune && alg <= 2 && !(warp_env && warp_env[0] == '1');
+  if (N == 64) return team ? emu_team<64>(a, alg) : (prune ? emu_alg<64, true>(a, alg) : emu_alg<64, false>(a, alg));
+  if (N == 32) return team ? emu_team<32>(a, alg) : (prune ? emu_alg<32, true>(a, alg) : emu_alg<32, false>(a, alg));
   return -2;
 }
 

@@ -187,3 +187,31 @@ def test_emulated_direct_masked(emu):
     assert worst <= MASK_PLANE_RTOL, worst
     bad = (np.abs(VF - VFo) > VF_ATOL).any(axis=0) & ~near_tie & ~sparse
     assert not bad.any(), np.abs(VF - VFo).max()
+
+
+@pytest.mark.parametrize("alg", ["fft", "zncc", "nsqecc"])
+@pytest.mark.parametrize("cfg", [((32, 32), (16, 16), (8, 8)), ((16, 16), (8, 8), (8, 8)), ((8, 12), (20, 18), (12, 12))])
+def test_emulated_team_and_warp_kernels_agree(emu, alg, cfg, monkeypatch):
+    """Pruned FFTCC/ZNCC/NSQECC run on the team kernel (one IA per team of N
+    threads); the one-warp-per-IA kernel (MQP_TUNE_PIV2D_WARP=1 on the GPU)
+    stays available.  Both emulations match the oracle and each other within
+    the FP32 plane tolerance."""
+    IS, SM, st = cfg
+    i1, i2, _ = synth.pair_2d_vortex(shape=(120, 112), seed_stream=27, core=30.0)
+    po = O.set_piv_parameters(corr_alg=alg, interSize=IS, searchMargin=SM, step=st, computeSN=True)
+    po.ndims = 2
+    VFo, SNo, Co = O.piv_single_pass(i1, i2, po, keep_corr=True)
+    out = {}
+    for mode in ("team", "warp"):
+        monkeypatch.setenv("MQP_EMU_PIV2D_WARP", "1" if mode == "warp" else "0")
+        VF, SN, PL = run_emu(emu, i1, i2, alg, IS, SM, st)
+        worst, near_tie = compare_planes(PL, Co, i1.shape, IS, SM, st)
+        assert worst <= PLANE_RTOL, (mode, worst)
+        bad = (np.abs(VF - VFo) > VF_ATOL).any(axis=0) & ~near_tie
+        assert not bad.any(), mode
+        assert (sn_ok(SN, SNo, sn_condition(Co, i1.shape, IS, SM, st)) | near_tie).all(), mode
+        out[mode] = PL
+    fin = np.isfinite(out["warp"])
+    assert np.array_equal(fin, np.isfinite(out["team"]))  # 0/0 lags (ZNCC in the padding) alike
+    scale = np.max(np.abs(out["warp"][fin]))
+    assert np.max(np.abs(out["team"][fin] - out["warp"][fin])) <= 2 * PLANE_RTOL * scale

@@ -42,6 +42,20 @@ def both(fn, VF, *a, **k):
     return conv(h), conv(d)
 
 
+def test_two_tuple_radius_on_3d_field_is_in_plane(gpu):
+    """localOp takes toDims3(radius)[1:N] (postprocessing.jl:65,85;
+    src/piv_parameters.jl:11): a 2-tuple radius on a 3D field is radius 0 along
+    axis 3, so the average never mixes z layers."""
+    VF = vf3d()
+    h, d = both(PP.average, VF, (2, 1))
+    assert np.allclose(h, PO.average((2, 1), VF), rtol=1e-13) and np.array_equal(d, h)
+    assert np.allclose(h, PO.average((2, 1, 0), VF), rtol=1e-13)
+    for z in range(VF.shape[3]):
+        assert np.allclose(h[..., z], PO.average((2, 1), VF[..., z]), rtol=1e-13)
+    h, d = both(PP.collectiveness, VF, (2, 2))
+    assert np.array_equal(h, PO.collectiveness((2, 2, 0), VF)) and np.array_equal(d, h)
+
+
 @pytest.mark.parametrize("which", ["2d", "3d"])
 def test_window_ops(which, vf2d):
     VF = vf2d[0] if which == "2d" else vf3d()
