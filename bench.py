@@ -56,9 +56,13 @@ def measured_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle reasons sampled every 200 ms while running."""
+    """nvidia-smi clocks/throttle reasons sampled every 50 ms while running.
+    Start it before the warm-up (nvidia-smi takes a moment to produce its
+    first sample); summary(t0, t1) keeps the samples taken between two
+    time.time() marks (the timed region), or all of them if that window
+    holds fewer than three."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -85,27 +89,31 @@ class ClockSampler:
             except Exception:
                 self.proc.kill()
 
-    def summary(self):
+    def summary(self, t0=None, t1=None):
         if self.proc is None or self.out is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        import datetime
         self.out.seek(0)
-        sm, smax, reasons = [], [], set()
+        rows = []
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in self.out:
             parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 10:
                 continue
             try:
-                sm.append(float(parts[1]))
-                smax.append(float(parts[2]))
+                ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                rows.append((ts, float(parts[2]), float(parts[3]),
+                             {n for n, v in zip(names, parts[6:10]) if v.lower().startswith("active")}))
             except ValueError:
                 continue
-            for n, v in zip(names, parts[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(smax) if smax else None,
-                "samples": len(sm), "reasons": sorted(reasons)}
+        window = "timed region"
+        sel = [r for r in rows if t0 is None or (t0 - 0.05 <= r[0] <= t1 + 0.05)]
+        if len(sel) < 3:
+            sel, window = rows, "warm-up and timed region (the timed region held fewer than 3 samples)"
+        reasons = set().union(*[r[3] for r in sel]) if sel else set()
+        return {"sm_mhz": statistics.median(r[1] for r in sel) if sel else None,
+                "sm_max_mhz": max(r[2] for r in sel) if sel else None,
+                "samples": len(sel), "window": window, "reasons": sorted(reasons)}
 
 
 def dist_env():
@@ -259,6 +267,7 @@ def run_ours(args):
     elif nd == 3:
         # launch tuning (results never depend on it): IAs per 3D chunk, timed here
         chunk3d, tuned = tune.autotune_chunk3d(ctx, step, stream, candidates=(1024, 2048, 4096, 8192, 16384))
+    clk = ClockSampler(local).__enter__()  # sampling from the warm-up on (nvidia-smi starts slowly)
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -267,13 +276,15 @@ def run_ours(args):
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
-        for k in range(args.steps):
-            flush.fill_(float(k))  # evict the inputs from L2 between steps (not timed)
-            ev[k][0].record(stream)
-            step()
-            ev[k][1].record(stream)
-        torch.cuda.synchronize()
+    t_on = time.time()
+    for k in range(args.steps):
+        flush.fill_(float(k))  # evict the inputs from L2 between steps (not timed)
+        ev[k][0].record(stream)
+        step()
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    t_off = time.time()
+    clk.__exit__()
     if world > 1:
         dist.barrier()
     prof = ctx.profile_read()
@@ -315,7 +326,8 @@ def run_ours(args):
         traffic = tr["dram_bytes_per_launch"] * n_ia / tr["ia_per_launch"]
     except Exception:
         pass
-    kname = "piv2d_kernel" if nd == 2 else "k3a_kernel + k3b_kernel + k3c_kernel (all chunks of one pass)"
+    kname = ("piv2d_team_kernel (one IA per team of 64 threads)" if nd == 2
+             else "k3a_kernel + k3b_kernel + k3c_kernel (all chunks of one pass)")
     roof = {"bound": "fp32", "kernel": kname, "achieved": achieved / 1e12, "peak": fp32_peak / 1e12,
             "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": traffic,
             "traffic_unit": f"bytes per pass (ncu dram__bytes_read+write, profiles/{tfile})",
@@ -344,13 +356,14 @@ def run_ours(args):
                         "h2d_bytes_per_step": int(2 * wl.image_bytes),
                         "d2h_bytes_per_step": int(n_ia * nd * 8)},
                 "gpu_launches": kernel_launches(wl, chunk3d or 1) * args.steps,
-                "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary(),
+                "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary(t_on, t_off),
                 "kernel_ms": {"piv": kern_ms, "integral_scans": prof["ms_integral"] / max(args.steps, 1)}}
-        print(json.dumps(line), flush=True)
+    del d1, d2, VF, flush
+    ctx.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
-    return 0
+    return line if rank == 0 else None
 
 
 # ---------------------------------------------------------------------------
@@ -424,9 +437,10 @@ def run_batch_plan_only(args):
 def run_batch(args):
     rank, _, world = dist_env()
     if rank != 0:  # a single-GPU workload: under a multi-rank launch rank 0 runs it alone
-        return 0
+        return None
     if args.plan_only:
-        return run_batch_plan_only(args)
+        run_batch_plan_only(args)
+        return None
     import torch
 
     import multi_quickpiv_b200 as mq
@@ -520,9 +534,8 @@ def run_batch(args):
                          "algorithmic_flop_per_step": flops,
                          "peak_source": f"148 SM x 128 FP32 lanes x 2 x sm_max_mhz ({src})"},
             "cpu_baseline": None, "clocks": clk.summary()}
-    print(json.dumps(line), flush=True)
     plan.close()
-    return 0
+    return line
 
 
 # ---------------------------------------------------------------------------
@@ -531,7 +544,7 @@ def run_batch(args):
 def run_serve(args):
     rank, _, world = dist_env()
     if rank != 0:  # a single-GPU workload: under a multi-rank launch rank 0 runs it alone
-        return 0
+        return None
     from multi_quickpiv_b200 import setPIVParameters, synth
     from multi_quickpiv_b200.serve import Server
     t0 = time.time()
@@ -612,8 +625,7 @@ def run_serve(args):
             "e2e": {"value": st["ia_per_s"], "unit": UNIT,
                     "h2d_bytes_per_step": int(2048 * 2048 * 4), "d2h_bytes_per_step": int(ia2 * 2 * 8)},
             "gpu_launches": None, "roofline": None, "cpu_baseline": None, "clocks": clk.summary()}
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 def main(argv=None):
@@ -633,14 +645,59 @@ def main(argv=None):
     ap.add_argument("--chunk3d", type=int, default=0, help="IAs per 3D chunk (0: autotuned in warm-up)")
     ap.add_argument("--plan-only", action="store_true",
                     help="batch64: time the plan alone (default options), e.g. for a launch list")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="vortex2048: skip the batch64, serve and shear3d summaries added to the line")
     args = ap.parse_args(argv)
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "batch64":
-        return run_batch(args)
-    if args.workload == "serve":
-        return run_serve(args)
-    return run_ours(args)
+        line = run_batch(args)
+    elif args.workload == "serve":
+        line = run_serve(args)
+    else:
+        line = run_ours(args)
+        if line is not None and args.workload == "vortex2048" and line["n_gpus"] == 1 and not args.no_extras:
+            line["extras"] = extras(args)
+    if line is not None:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def extras(args):
+    """The other configured workloads, measured in the same run and summarised
+    beside the headline line: the 512x512x256 3D FFTCC pass, the 64-pair
+    batch (plan vs one PIV call per pair) and serving (p50/p99 latency vs the
+    plain per-request path).  Each runs with its own reduced step count; a
+    failure is reported in its entry and never fails the line."""
+    import copy
+
+    import torch
+    out = {}
+    jobs = [("shear3d", lambda a: run_ours(a), dict(workload="shear3d", steps=max(5, args.steps // 4), warmup=3,
+                                                    no_cpu=True, chunk3d=0)),
+            ("batch64", lambda a: run_batch(a), dict(workload="batch64", steps=max(4, args.steps // 5), warmup=3)),
+            ("serve", lambda a: run_serve(a), dict(workload="serve", steps=max(200, args.steps)))]
+    for name, fn, over in jobs:
+        a = copy.copy(args)
+        for k, v in over.items():
+            setattr(a, k, v)
+        t0 = time.time()
+        try:
+            ln = fn(a)
+            keep = ("value", "ms_per_step", "steps", "e2e", "config", "speedup_vs_plain", "plain_path",
+                    "latency_ms", "plain_path_latency_ms", "admitted_while_busy", "completed", "failed",
+                    "gpu_launches", "clocks")
+            ent = {k: ln[k] for k in keep if k in ln}
+            if ln.get("roofline"):
+                ent["roofline"] = {k: ln["roofline"][k] for k in ("achieved", "peak", "unit", "frac", "kernel_ms")
+                                   if k in ln["roofline"]}
+        except Exception as e:  # reported, never fatal
+            ent = {"error": f"{type(e).__name__}: {e}"}
+        ent["wall_s"] = time.time() - t0
+        out[name] = ent
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+    return out
 
 
 if __name__ == "__main__":

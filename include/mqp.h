@@ -329,6 +329,58 @@ MQP_API int mqp_postprocess(mqp_ctx* ctx, const mqp_post_params* p, const mqp_fi
                             const uint8_t* mask, double* out, float* outf, uint8_t* mask_out);
 
 /*
+ * Pseudo-trajectories over a vector-field time series: PIVtrajectories and
+ * PIVtrajectories_grid (src/postprocessing/postprocessing.jl:988-1120).  The
+ * field components U, V (and W in 3D) are column-major arrays of `dtype`
+ * with extents (dims[0], dims[1][, dims[2]], frames), as the reference's 4-D
+ * U, V, W (a 2-D field over time, U and V only, is this build's extension).
+ * Each particle starts at an integer position of the sampling region, moves
+ * by the displacement sampled at its rounded position (Float32 positions,
+ * round to nearest with ties to even, the reference's round(Int64, x)) and
+ * stops, its remaining positions frozen, when the rounded position leaves
+ * the field.  Positions are 1-based like the reference's.  Outputs TY, TX
+ * (TZ) are Float32 (numT, numpoints) column-major, numT = T1 - T0.
+ *
+ *  - T0, T1: 1-based frames; frames T0 .. T1-1 must exist (the last step
+ *    samples frame T1-1, as the reference does).
+ *  - sub_lo[d] > sub_hi[d] selects the reference's default 2 : dims[d]-1;
+ *    otherwise the 1-based inclusive range sub_lo[d] : sub_hi[d] (grid: with
+ *    step[d]).
+ *  - grid = 0: numpoints random starting positions.  Julia's `rand` stream is
+ *    not reproducible outside Julia, so a counter-based generator replaces
+ *    it: start along axis d = lo + step * (splitmix64(seed + (3p+d+1) *
+ *    0x9E3779B97F4A7C15) mod len).  grid = 1: every point of the sampling
+ *    grid, y fastest (the reference's loop order); numpoints is ignored and
+ *    mqp_traj_count gives the count.
+ *  - scale[d] multiplies component d (in FP64, then rounded to Float32, as
+ *    Julia's Float32(scale * U[...]) with a Float64 field).
+ *  - A non-finite rounded position counts as leaving the field (the reference
+ *    throws InexactError there).
+ */
+typedef struct mqp_traj_params {
+  int32_t ndims;      /* 2 or 3 */
+  int64_t dims[3];    /* grid extents of one frame */
+  int64_t frames;     /* frames in the arrays */
+  int32_t T0, T1;
+  int64_t sub_lo[3], sub_hi[3], step[3];
+  double scale[3];
+  int32_t grid;
+  int64_t numpoints;
+  uint64_t seed;
+  int32_t reserved[8];
+} mqp_traj_params;
+
+/* Particles a request follows (numpoints, or the grid's point count). */
+MQP_API int mqp_traj_count(const mqp_traj_params* p, int64_t* numpoints_out);
+/* On device arrays, enqueued on `stream` (NULL = legacy default stream). */
+MQP_API int mqp_trajectories_device(mqp_ctx* ctx, const mqp_traj_params* p, int dtype, const void* d_U,
+                                    const void* d_V, const void* d_W, float* d_TY, float* d_TX, float* d_TZ,
+                                    void* stream);
+/* The same on host arrays (only frames T0 .. T1-1 are copied; blocks). */
+MQP_API int mqp_trajectories(mqp_ctx* ctx, const mqp_traj_params* p, int dtype, const void* U, const void* V,
+                             const void* W, float* TY, float* TX, float* TZ);
+
+/*
  * Allocation-free 2D PIV.  No counterpart in the reference: it exists for
  * callers that cannot allocate GPU memory when they compute a vector field
  * (code running under a framework that owns all device memory through its

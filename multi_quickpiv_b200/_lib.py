@@ -111,6 +111,24 @@ class MqpPostParams(C.Structure):
     ]
 
 
+class MqpTrajParams(C.Structure):
+    _fields_ = [
+        ("ndims", C.c_int32),
+        ("dims", C.c_int64 * 3),
+        ("frames", C.c_int64),
+        ("T0", C.c_int32),
+        ("T1", C.c_int32),
+        ("sub_lo", C.c_int64 * 3),
+        ("sub_hi", C.c_int64 * 3),
+        ("step", C.c_int64 * 3),
+        ("scale", C.c_double * 3),
+        ("grid", C.c_int32),
+        ("numpoints", C.c_int64),
+        ("seed", C.c_uint64),
+        ("reserved", C.c_int32 * 8),
+    ]
+
+
 (MQP_POST_MAGNITUDES, MQP_POST_AVERAGE, MQP_POST_SIMILARITY_AVG, MQP_POST_COLLECTIVENESS, MQP_POST_TH_MASK,
  MQP_POST_STD_MASK, MQP_POST_REPLACE, MQP_POST_LOCAL_MAGNITUDE, MQP_POST_MATLAB_DIVERGENCE,
  MQP_POST_DIVERGENCE) = range(10)
@@ -153,6 +171,11 @@ SIGNATURES = {
                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "mqp_postprocess": (C.c_int, [C.c_void_p, C.POINTER(MqpPostParams), C.POINTER(MqpField), C.c_void_p,
                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "mqp_traj_count": (C.c_int, [C.POINTER(MqpTrajParams), C.POINTER(C.c_int64)]),
+    "mqp_trajectories_device": (C.c_int, [C.c_void_p, C.POINTER(MqpTrajParams), C.c_int, C.c_void_p, C.c_void_p,
+                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "mqp_trajectories": (C.c_int, [C.c_void_p, C.POINTER(MqpTrajParams), C.c_int, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 
 _lib = None

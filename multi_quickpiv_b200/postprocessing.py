@@ -377,3 +377,93 @@ def multiscale_divergence(radii, VF, min_value=0.2, normalize=True, min_speed=0,
         sc = xp.where(uc, r0, sc)
         mxc = xp.where(uc, c, mxc)
     return sd, mxd, sc, mxc
+
+
+# ---------------------------------------------------------------------------
+# pseudo-trajectories (postprocessing.jl:988-1120)
+# ---------------------------------------------------------------------------
+def _traj_range(r):
+    """A sampling range as (lo, hi), 1-based inclusive like Julia's lo:hi:
+    None (or an empty range) selects the reference's default 2:dims-1; a
+    (lo, hi) pair is taken as is; a Python range(a, b) means a:b-1."""
+    if r is None:
+        return 1, 0
+    if isinstance(r, range):
+        return (r.start, r.stop - 1) if len(r) else (1, 0)
+    lo, hi = r
+    return int(lo), int(hi)
+
+
+def _trajectories(comps, T0, T1, numpoints, subregion, scale, grid, step, seed, context):
+    nd = len(comps)
+    shape = tuple(comps[0].shape)
+    if any(tuple(c.shape) != shape for c in comps) or len(shape) != nd + 1:
+        raise AssertionError("U, V(, W) must be (d1, d2[, d3], frames) arrays of the same size")
+    p = _lib.MqpTrajParams()
+    p.ndims = nd
+    for d in range(nd):
+        p.dims[d] = int(shape[d])
+    p.frames = int(shape[nd])
+    p.T0, p.T1 = int(T0), int(T1)
+    sub = subregion if subregion is not None else (None,) * nd
+    sc = (scale,) * 3 if np.isscalar(scale) else tuple(scale) + (1,) * (3 - len(scale))
+    st = (step,) * 3 if np.isscalar(step) else tuple(step) + (1,) * (3 - len(step))
+    for d in range(nd):
+        p.sub_lo[d], p.sub_hi[d] = _traj_range(sub[d])
+        p.step[d] = int(st[d])
+        p.scale[d] = float(sc[d])
+    p.grid = int(bool(grid))
+    p.numpoints = int(numpoints)
+    p.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
+    lib = _lib.load()
+    npts = C.c_int64()
+    _lib.check(lib.mqp_traj_count(C.byref(p), C.byref(npts)), None)
+    n, numT = int(npts.value), int(T1) - int(T0)
+    if _is_torch(comps[0]):
+        import torch
+        dev = comps[0].device
+        ctx = context or _lib.default_context(dev.index or 0)
+        dt = torch.float64 if any(c.dtype == torch.float64 for c in comps) else torch.float32
+        xs = [_colmajor_torch(c.to(dt)) for c in comps]
+        outs = [_torch_empty_colmajor((numT, n), torch.float32, dev) for _ in range(nd)]
+        vp = lambda t: None if t is None else C.c_void_p(t.data_ptr())
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        rc = ctx.lib.mqp_trajectories_device(ctx.handle, C.byref(p), _lib.MQP_F64 if dt == torch.float64 else _lib.MQP_F32,
+                                             vp(xs[0]), vp(xs[1]), vp(xs[2] if nd == 3 else None), vp(outs[0]),
+                                             vp(outs[1]), vp(outs[2] if nd == 3 else None), C.c_void_p(stream))
+        _lib.check(rc, ctx.handle)
+    else:
+        ctx = context or _lib.default_context(0)
+        dt = np.float64 if any(np.asarray(c).dtype == np.float64 for c in comps) else np.float32
+        xs = [np.asfortranarray(np.asarray(c, dtype=dt)) for c in comps]
+        outs = [np.zeros((numT, n), dtype=np.float32, order="F") for _ in range(nd)]
+        ptr = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)
+        rc = ctx.lib.mqp_trajectories(ctx.handle, C.byref(p), _lib.MQP_F64 if dt == np.float64 else _lib.MQP_F32,
+                                      ptr(xs[0]), ptr(xs[1]), ptr(xs[2] if nd == 3 else None), ptr(outs[0]),
+                                      ptr(outs[1]), ptr(outs[2] if nd == 3 else None))
+        _lib.check(rc, ctx.handle)
+    return tuple(outs) + ((None,) if nd == 2 else ())
+
+
+def PIVtrajectories(U, V, W, T0, T1, numpoints, subregion=None, scale=(1, 1, 1), seed=0, context=None):
+    """PIVtrajectories(U, V, W, T0, T1, numpoints; subregion, scale)
+    (postprocessing.jl:988-1050) on the GPU: numpoints particles from random
+    integer positions of the sampling region, followed through frames T0 (1-based)
+    onwards; returns (TrajectoriesY, TrajectoriesX, TrajectoriesZ), Float32
+    arrays of shape (T1 - T0, numpoints) with 1-based positions.  U, V, W are
+    (d1, d2, d3, frames) arrays (NumPy or torch CUDA); W = None follows a 2D
+    field over time (then TrajectoriesZ is None).  The starting positions come
+    from a counter-based generator seeded by `seed` (Julia's rand stream cannot
+    be reproduced outside Julia)."""
+    comps = [U, V] + ([W] if W is not None else [])
+    return _trajectories(comps, T0, T1, numpoints, subregion, scale, False, 1, seed, context)
+
+
+def PIVtrajectories_grid(U, V, W, T0, T1, numpoints=0, subregion=None, step=(1, 1, 1), scale=(1, 1, 1),
+                         context=None):
+    """PIVtrajectories_grid(U, V, W, T0, T1, numpoints; subregion, step, scale)
+    (postprocessing.jl:1055-1120) on the GPU: one particle per point of the
+    sampling grid (step apart, y fastest); numpoints is unused, as in the
+    reference."""
+    comps = [U, V] + ([W] if W is not None else [])
+    return _trajectories(comps, T0, T1, numpoints, subregion, scale, True, step, 0, context)

@@ -341,3 +341,77 @@ def average_NDT(radius1, radius2, VF):
     nd = VF.ndim - 1
     r = _radii(radius1, nd - 1) + (int(radius2),)
     return average(r, VF)
+
+
+# --------------------------------------------------------------------------
+# pseudo-trajectories (postprocessing.jl:988-1120)
+# --------------------------------------------------------------------------
+_M64 = (1 << 64) - 1
+
+
+def traj_hash(seed, p, d):
+    """The random variant's starting-position generator (a build-defined
+    replacement for Julia's rand): splitmix64's finaliser of
+    seed + (3p + d + 1) * 0x9E3779B97F4A7C15, in 64-bit unsigned arithmetic."""
+    z = (seed + (3 * p + d + 1) * 0x9E3779B97F4A7C15) & _M64
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & _M64
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & _M64
+    return z ^ (z >> 31)
+
+
+def pivtrajectories(comps, T0, T1, numpoints=0, subregion=None, scale=(1, 1, 1), grid=False, step=(1, 1, 1),
+                    seed=0):
+    """PIVtrajectories / PIVtrajectories_grid (postprocessing.jl:988-1120),
+    one particle at a time as the reference's loop: comps = [U, V(, W)],
+    (d1, d2[, d3], frames) arrays; subregion per axis as (lo, hi) 1-based
+    inclusive, (1, 0) = the default 2:dims-1.  Positions are Float32 and
+    1-based; the displacement is sampled at round(Int64, pos) (ties to even,
+    :1037/:1104) and the trajectory freezes once that leaves the field
+    (:1040-1045).  Starting positions: the grid in the reference's loop order
+    (y fastest, :1070), or traj_hash for the random variant (the reference
+    calls rand, :1009)."""
+    nd = len(comps)
+    dims = comps[0].shape[:nd]
+    numT = T1 - T0
+    sub = subregion if subregion is not None else [(1, 0)] * nd
+    sc = (scale,) * 3 if np.isscalar(scale) else tuple(scale)
+    st = (step,) * 3 if np.isscalar(step) else tuple(step)
+    lo, ln, stp = [], [], []
+    for d in range(nd):
+        a, b = sub[d]
+        if a > b:
+            a, b = 2, dims[d] - 1
+        s_ = st[d] if grid else 1
+        lo.append(a)
+        stp.append(s_)
+        ln.append((b - a) // s_ + 1)
+    n = int(np.prod(ln)) if grid else int(numpoints)
+    out = [np.zeros((numT, n), dtype=np.float32, order="F") for _ in range(nd)]
+
+    def sample(q, frame1):
+        return [np.float32(float(sc[d]) * float(comps[d][tuple(x - 1 for x in q) + (frame1 - 1,)]))
+                for d in range(nd)]
+
+    for p in range(n):
+        if grid:
+            rem, s = p, []
+            for d in range(nd):
+                s.append(lo[d] + stp[d] * (rem % ln[d]))
+                rem //= ln[d]
+        else:
+            s = [lo[d] + stp[d] * (traj_hash(seed, p, d) % ln[d]) for d in range(nd)]
+        pos = [np.float32(x) for x in s]
+        for d in range(nd):
+            out[d][0, p] = pos[d]
+        dv = sample(s, T0)
+        for t in range(1, numT):
+            pos = [np.float32(pos[d] + dv[d]) for d in range(nd)]
+            for d in range(nd):
+                out[d][t, p] = pos[d]
+            r = [np.rint(x) for x in pos]
+            if any(not (1 <= x <= dims[d]) for d, x in enumerate(r)):
+                for d in range(nd):
+                    out[d][t:, p] = out[d][t - 1, p]
+                break
+            dv = sample([int(x) for x in r], T0 + t)
+    return tuple(out)

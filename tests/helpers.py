@@ -93,4 +93,7 @@ def sn_ok(SN, SNo, kappa=None):
     except where the IA's own condition number (sn_condition) times the plane
     tolerance is larger.  Without kappa the plain 1e-4 applies."""
     rel = SN_RTOL if kappa is None else np.maximum(SN_RTOL, PLANE_RTOL * np.asarray(kappa))
-    return (np.abs(SN - SNo) <= rel * np.abs(SNo)) | ~np.isfinite(SNo)
+    diff = np.abs(SN - SNo)
+    with np.errstate(invalid="ignore"):  # an infinite kappa times SN = 0 (a skipped IA)
+        within = diff <= rel * np.abs(SNo)
+    return (diff == 0) | within | ~np.isfinite(SNo)

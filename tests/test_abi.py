@@ -32,7 +32,8 @@ def test_library_exports_every_declared_symbol():
                                       ("mqp_field", "MqpField"), ("mqp_post_params", "MqpPostParams"),
                                       ("mqp_batch_item", "MqpBatchItem"), ("mqp_batch_options", "MqpBatchOptions"),
                                       ("mqp_server_options", "MqpServerOptions"),
-                                      ("mqp_server_stats", "MqpServerStats")])
+                                      ("mqp_server_stats", "MqpServerStats"),
+                                      ("mqp_traj_params", "MqpTrajParams")])
 def test_abi_version_and_struct_layout(tmp_path, cname, py):
     """Each ctypes mirror matches the C layout (size and every field offset),
     checked by compiling a probe against include/mqp.h."""
