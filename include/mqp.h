@@ -85,7 +85,8 @@ typedef struct mqp_params {
   double threshold;        /* skip IA when threshold >= 0 and maxval(IA) < threshold */
   double mask_threshold;   /* masked PIV: skip when > 0 and maxval(mask IA) < it */
   double ovp_th;           /* carried for completeness; unused by the reference kernels */
-  int32_t refine;          /* 0: multipass re-runs scale 1 (the reference); 1: predictor refinement */
+  int32_t refine;          /* 0: multipass re-runs scale 1 (the reference); 1: whole-pixel predictor
+                              refinement; 2: refinement with window deformation (no masks) */
   int32_t reserved[7];
 } mqp_params;
 

@@ -296,7 +296,42 @@ int run_multipass(mqp_ctx* ctx, const mqp_params* p, const void* d1, const void*
       outVF = (double*)b.ptr;
     }
     const int32_t* dpred = nullptr;
-    if (prevVF && pb.n_ia > 0) {
+    const bool deform = p->refine == 2 && prevVF && pb.n_ia > 0 && prev.n_ia > 0;
+    const void* in1 = d1;
+    const void* in2 = d2;
+    mqp::DeformArgs da;
+    if (deform) {
+      // the images resampled around the dense predictor of the previous pass
+      // (mqp_deform.cuh); this pass measures the residual
+      memset(&da, 0, sizeof(da));
+      da.nd = ndims;
+      da.dtype = dtype;
+      for (int d = 0; d < 3; ++d) da.dims[d] = d < ndims ? dims[d] : 1;
+      const size_t img_b = (size_t)(da.dims[0] * da.dims[1] * da.dims[2]) * elem_size(dtype);
+      if ((e = ctx->def1.ensure(img_b)) != cudaSuccess || (e = ctx->def2.ensure(img_b)) != cudaSuccess)
+        return cuda_fail(ctx, e, "deformed image buffers");
+      da.img1 = d1;
+      da.img2 = d2;
+      da.out1 = ctx->def1.ptr;
+      da.out2 = ctx->def2.ptr;
+      da.VFc = prevVF;
+      for (int d = 0; d < ndims; ++d) {
+        da.vf_c[d] = (int)prev.vf[d];
+        da.isz_c[d] = prev.IS[d];
+        da.st_c[d] = prev.st[d];
+        da.vf_f[d] = (int)pb.vf[d];
+        da.isz_f[d] = pb.IS[d];
+        da.st_f[d] = pb.st[d];
+      }
+      da.threshold = p->threshold;
+      {
+        ProfileScope ps(ctx, s, 2, 0);
+        if ((e = mqp::launch_deform(da, s)) != cudaSuccess) return cuda_fail(ctx, e, "deform kernel");
+      }
+      in1 = da.out1;
+      in2 = da.out2;
+    }
+    if (prevVF && pb.n_ia > 0 && !deform && p->refine != 2) {
       if ((e = ctx->pred.ensure((size_t)pb.n_ia * ndims * sizeof(int32_t))) != cudaSuccess)
         return cuda_fail(ctx, e, "predictor buffer");
       mqp::PredArgs pa;
@@ -321,9 +356,14 @@ int run_multipass(mqp_ctx* ctx, const mqp_params* p, const void* d1, const void*
     if (pb.n_ia > 0) {
       const int64_t b0 = level == 0 ? ia_begin : 0, b1 = level == 0 ? ia_end : pb.n_ia;
       double* pl = level == 0 ? dplanes : nullptr;
-      rc = ndims == 3 ? run_pass_3d(ctx, pb, p, d1, d2, dmask, dskip, dtype, outVF, outSN, dpred, pl, b0, b1, s)
-                      : run_pass_2d(ctx, pb, p, d1, d2, dmask, dskip, dtype, outVF, outSN, dpred, pl, b0, b1, s);
+      rc = ndims == 3 ? run_pass_3d(ctx, pb, p, in1, in2, dmask, dskip, dtype, outVF, outSN, dpred, pl, b0, b1, s)
+                      : run_pass_2d(ctx, pb, p, in1, in2, dmask, dskip, dtype, outVF, outSN, dpred, pl, b0, b1, s);
       if (rc != MQP_OK) return rc;
+      if (deform) {
+        da.VF = outVF;
+        ProfileScope ps(ctx, s, 2, 0);
+        if ((e = mqp::launch_deform_add(da, s)) != cudaSuccess) return cuda_fail(ctx, e, "deform add kernel");
+      }
     }
     prev = pb;
     prevVF = outVF;

@@ -152,6 +152,8 @@ int mqp_batch_plan_create(mqp_ctx* ctx, const mqp_batch_item* items, int32_t n_i
     if (!it.img1 || !it.img2) return fail(ctx, MQP_ERR_INVALID, who + "null image pointer");
     if (it.dtype != MQP_F32 && it.dtype != MQP_F64) return fail(ctx, MQP_ERR_INVALID, who + "dtype must be MQP_F32 or MQP_F64");
     const bool masked = it.mask != nullptr;
+    if (it.params.refine == 2 && it.params.multipass > 1)
+      return fail(ctx, MQP_ERR_UNSUPPORTED, who + "batch plans run the whole-pixel refinement (refine = 1), not deformation");
     ip.levels = (it.params.refine && it.params.multipass > 1) ? it.params.multipass : 1;
     if (ip.levels > 16) return fail(ctx, MQP_ERR_INVALID, who + "multipass too large");
     ip.lev.resize(ip.levels);

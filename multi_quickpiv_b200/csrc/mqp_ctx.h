@@ -47,6 +47,7 @@ struct mqp_ctx {
   std::mutex mu;
   mqp_host::DevBuf img1, img2, mask, mask_skip, II1, IIg, IIg2, VF, SN, pred, planes, status, iscratch, scratch3d;
   mqp_host::DevBuf passVF[2];  // vectors of the coarse passes of a multi-pass refinement
+  mqp_host::DevBuf def1, def2;  // deformed images of the deforming refinement
   mqp_host::DevBuf post_in, post_mask, post_out, post_outf, post_mask_out, post_scratch;
   mqp_host::DevBuf traj_in, traj_out;  // host-array pseudo-trajectories
   // host-array 2D path: copy-in and copy-out streams, events of its pieces
@@ -139,6 +140,9 @@ inline int resolve(mqp_ctx* ctx, const mqp_params* p, int ndims, const int64_t d
                 "ERROR: all gaussian_displacement should be unpadded (stored unpadded must be true; "
                 "setPIVParameters stores the good_pad argument there)");
   if (p->multipass < 1) return fail(ctx, MQP_ERR_INVALID, "multipass must be >= 1");
+  if (p->refine < 0 || p->refine > 2) return fail(ctx, MQP_ERR_INVALID, "refine must be 0, 1 or 2");
+  if (p->refine == 2 && masked && p->multipass > 1)
+    return fail(ctx, MQP_ERR_UNSUPPORTED, "window deformation (refine = 2) does not take masks");
   pb.ndims = ndims;
   pb.alg = masked ? mqp::ALG_MASK_NSQECC : p->corr_alg;
   if (!masked && (p->corr_alg < 0 || p->corr_alg > 2))

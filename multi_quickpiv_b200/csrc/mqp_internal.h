@@ -9,6 +9,7 @@
 #include "mqp_piv2d.cuh"
 #include "mqp_piv3d.cuh"
 #include "mqp_multipass.cuh"
+#include "mqp_deform.cuh"
 #include "mqp_post.cuh"
 #include "mqp_direct.cuh"
 
@@ -104,6 +105,10 @@ cudaError_t launch_piv3d(const Piv3dArgs& a, int alg, long long chunk, cudaStrea
 
 // Multi-pass refinement: the fine pass's predictor from the coarse vectors.
 cudaError_t launch_predictor(const PredArgs& a, cudaStream_t s);
+// Deforming refinement: both images resampled around the dense predictor
+// (a.out1/out2), and the predictor added back to the fine pass's vectors.
+cudaError_t launch_deform(const DeformArgs& a, cudaStream_t s);
+cudaError_t launch_deform_add(const DeformArgs& a, cudaStream_t s);
 
 // Vector-field post-processing (one op); scratch holds post_scratch_bytes().
 cudaError_t launch_post(const PostArgs& a, double* scratch, cudaStream_t s);

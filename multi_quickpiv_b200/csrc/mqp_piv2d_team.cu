@@ -175,9 +175,7 @@ __device__ __forceinline__ void piv2d_team_ia(const Piv2dArgs& a, long long ia, 
   // ---- phase 1: F rows (thread pairs, half warp-uniform at N = 64), G rows ----
   double vmax = -INFINITY, sumsq = 0.0;
   {
-    const int hh = tid / M, q = tid % M;
-    if (hh == 0) team_f_row<N, T, ZN, 0>(a, g, sc.meanF, q, F, vmax, sumsq);
-    else team_f_row<N, T, ZN, 1>(a, g, sc.meanF, q, F, vmax, sumsq);
+    team_f_row<N, T, ZN>(a, g, sc.meanF, tid % M, tid / M, F, vmax, sumsq);
   }
   team_g_row<N, T, ZN>(a, g, (float)sc.meanG, tid, G);
   // skip_inter_region (src/utils/piv_ops.jl:134-157) needs the IA maximum
@@ -222,9 +220,7 @@ __device__ __forceinline__ void piv2d_team_ia(const Piv2dArgs& a, long long ia, 
 
   // ---- phase 2: spectrum columns, thread pair (u, half) ----
   {
-    const int h = tid / M, u = tid % M;
-    if (h == 0) team_phase2<N, 0>(u, G, F, sync);
-    else team_phase2<N, 1>(u, G, F, sync);
+    team_phase2<N>(tid % M, tid / M, G, F, sync);
   }
   sync();
 
@@ -237,10 +233,7 @@ __device__ __forceinline__ void piv2d_team_ia(const Piv2dArgs& a, long long ia, 
     const int hh = tid / M, j = tid % M;
     for (int b = 0; b < paired; b += M) {
       const int s1 = b + j;
-      if (s1 < paired) {
-        if (hh == 0) team_phase3_row<N, 0>(s1, P1, P2, G, cc, scale);
-        else team_phase3_row<N, 1>(s1, P1, P2, G, cc, scale);
-      }
+      if (s1 < paired) team_phase3_row<N>(s1, hh, P1, P2, G, cc, scale);
     }
     if (tail) {
       for (int s2 = tid; s2 < P2; s2 += N) cc[(P1 - 1) + P1 * s2] = team_tail_value<N>(G, tw, s2) * scale;

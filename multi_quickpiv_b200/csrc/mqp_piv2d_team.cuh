@@ -25,7 +25,11 @@
 // line's transform with half the registers of one thread doing all of it,
 // and twice the warps fit on an SM (a team holds about 25 KB of shared
 // memory at N = 64: nine IAs, eighteen warps per SM).  The split half is
-// uniform across a warp at N = 64 (warp 0 takes half 0, warp 1 half 1).
+// uniform across a warp at N = 64 (warp 0 takes half 0, warp 1 half 1); the
+// two halves share every transform body and differ only in the short steps
+// around it, so the kernel's code stays small enough for the instruction
+// cache (a version with one copy of each phase per half stalled on
+// instruction fetch).
 #pragma once
 
 #include "mqp_piv2d.cuh"
@@ -100,47 +104,19 @@ MQP_HD MQP_FI void team_g_row(const Piv2dArgs& a, const IAGeom& g, float mg, int
 }
 
 // F row q (interrogation window row, zero past IS1; minus the IA mean for
-// ZNCC), half HH of its length-M complex FFT.  The row's packed input
+// ZNCC), half hh of its length-M complex FFT.  The row's packed input
 // z[n] = x[2n] + i x[2n+1] is zero for n >= M/2 (F is at most M wide), so the
 // first decimation-in-frequency stage reduces to Z[2k] = FFT_{M/2}(z)[k] and
 // Z[2k+1] = FFT_{M/2}(z W_M^n)[k].  Bin k' of the real transform needs Z[k']
 // and Z[M-k'], which share k''s parity, so this thread finishes the bins of
-// parity HH and writes them to F[k' * FS + q].  The HH = 0 thread also takes
+// parity hh and writes them to F[k' * FS + q].  The hh = 0 thread also takes
 // the raw maximum (skip test) and the FP64 sum of squares of the values.
-template <int N, typename T, bool ZNCC, int HH>
-MQP_HD MQP_FI void team_f_row(const Piv2dArgs& a, const IAGeom& g, double meanF, int q, float2* F, double& vmax,
-                              double& sumsq) {
-  mqp_no_hoist();
+// Only the twiddle and the bin finishing depend on hh, so the transform
+// body exists once for both halves (instruction-cache footprint).
+template <int N, int HH>
+MQP_HD MQP_FI void team_f_bins(int q, const float2 (&w)[N / 4], float2* F) {
   constexpr int M = N / 2, Q = M / 2, FS = TeamLayout<N>::FS;
-  if (q >= a.IS1) {
-#pragma unroll
-    for (int k = 0; k < Q; ++k) F[(2 * k + HH) * FS + q] = make_float2(0.f, 0.f);
-    return;
-  }
-  const T* src = reinterpret_cast<const T*>(a.img1) + ((long long)(g.ir1 + q) + (long long)a.H * g.ir2);
-  const long long H = a.H;
-  float2 w[Q];
-#pragma unroll
-  for (int n = 0; n < Q; ++n) {
-    float v[2];
-#pragma unroll
-    for (int e = 0; e < 2; ++e) {
-      const int x = 2 * n + e;
-      v[e] = 0.f;
-      if (x < a.IS2) {
-        const T r = ldg_px<T>(src, H * x);
-        const double val = (double)r - meanF;
-        if (HH == 0) {
-          vmax = (double)r > vmax ? (double)r : vmax;
-          sumsq += val * val;
-        }
-        v[e] = (float)val;
-      }
-    }
-    w[n] = make_float2(v[0], v[1]);
-    if (HH == 1) w[n] = rotate<M, false>(w[n], n);
-  }
-  fft_reg<Q, false>(w);  // Z[2k + HH] = w[fpos<Q>(k)]
+  mqp_no_hoist();
 #pragma unroll
   for (int k = 0; k < Q; ++k) {
     const int kp = 2 * k + HH;  // bin of the real transform
@@ -158,6 +134,45 @@ MQP_HD MQP_FI void team_f_row(const Piv2dArgs& a, const IAGeom& g, double meanF,
   }
 }
 
+template <int N, typename T, bool ZNCC>
+MQP_HD MQP_FI void team_f_row(const Piv2dArgs& a, const IAGeom& g, double meanF, int q, int hh, float2* F,
+                              double& vmax, double& sumsq) {
+  constexpr int M = N / 2, Q = M / 2, FS = TeamLayout<N>::FS;
+  if (q >= a.IS1) {
+    for (int k = 0; k < Q; ++k) F[(2 * k + hh) * FS + q] = make_float2(0.f, 0.f);
+    return;
+  }
+  const T* src = reinterpret_cast<const T*>(a.img1) + ((long long)(g.ir1 + q) + (long long)a.H * g.ir2);
+  const long long H = a.H;
+  float2 w[Q];
+#pragma unroll
+  for (int n = 0; n < Q; ++n) {
+    float v[2];
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const int x = 2 * n + e;
+      v[e] = 0.f;
+      if (x < a.IS2) {
+        const T r = ldg_px<T>(src, H * x);
+        const double val = (double)r - meanF;
+        if (hh == 0) {
+          vmax = (double)r > vmax ? (double)r : vmax;
+          sumsq += val * val;
+        }
+        v[e] = (float)val;
+      }
+    }
+    w[n] = make_float2(v[0], v[1]);
+  }
+  if (hh) {
+#pragma unroll
+    for (int n = 1; n < Q; ++n) w[n] = rotate<M, false>(w[n], n);
+  }
+  fft_reg<Q, false>(w);  // Z[2k + hh] = w[fpos<Q>(k)]
+  if (hh) team_f_bins<N, 1>(q, w, F);
+  else team_f_bins<N, 0>(q, w, F);
+}
+
 // ---------------------------------------------------------------------------
 // phase 2: spectrum column u, half H2 (bins k1 = 2m + H2 along dim 1)
 // ---------------------------------------------------------------------------
@@ -169,72 +184,111 @@ MQP_HD MQP_FI void team_f_row(const Piv2dArgs& a, const IAGeom& g, double meanF,
 // combines the two halves' inverses A0[s] + W_N^-s A1[s] (s < M) and
 // A0[s] - W_N^-s A1[s] (s + M).  On return G[u] holds A0 in slots 0..M-1 and
 // W_N^-s A1[s] in slots M..N-1.
-// first part: G column u folded into half H2 and transformed (x, registers)
+// The three transforms of a column half (G forward, F forward, the product's
+// inverse through the forward transform of its conjugate) run as stages
+// st = 0, 1, 2 of one loop around a single FFT body; team_p2_pre loads the
+// stage's input into t, team_p2_post consumes the transform.  Between the
+// transform and the post of stage 0 the team synchronises (every column has
+// been read before the halves are written back into it).
 template <int N, int H2>
-MQP_HD MQP_FI void team_p2_fold(int u, const float2* G, float2 (&x)[N / 2]) {
+MQP_HD MQP_FI void team_p2_fold(const float2* Gc, float2 (&t)[N / 2]) {
   constexpr int M = N / 2;
-  const float2* Gc = G + u * TeamLayout<N>::GS;
+  mqp_no_hoist();
 #pragma unroll
   for (int n = 0; n < M; ++n) {
     const float2 a0 = Gc[n], a1 = Gc[n + M];
-    x[n] = H2 ? rotate<N, false>(csub(a0, a1), n) : cadd(a0, a1);
+    t[n] = H2 ? rotate<N, false>(csub(a0, a1), n) : cadd(a0, a1);
   }
-  fft_reg<M, false>(x);  // G^ bin 2m + H2 at x[fpos<M>(m)]
 }
 
-// second part (after every thread of the team has folded its column): G^
-// back to the column's half, F's half, the product and its inverse
 template <int N, int H2>
-MQP_HD MQP_FI void team_p2_corr(int u, float2* G, const float2* F, const float2 (&x)[N / 2]) {
+MQP_HD MQP_FI void team_p2_fload(const float2* Fc, float2 (&t)[N / 2]) {
   constexpr int M = N / 2;
-  float2* Gc = G + u * TeamLayout<N>::GS;
-  const float2* Fc = F + u * TeamLayout<N>::FS;
-#pragma unroll
-  for (int m = 0; m < M; ++m) Gc[H2 * M + m] = x[fpos<M>(m)];
-  // keep the stores here: moved later they would hold x live across the F work
   mqp_no_hoist();
-  float2 f[M];
 #pragma unroll
-  for (int n = 0; n < M; ++n) f[n] = H2 ? rotate<N, false>(Fc[n], n) : Fc[n];
-  fft_reg<M, false>(f);  // F^ bin 2m + H2 at f[fpos<M>(m)]
-  // t = conj(conj(F^) G^), natural order; column 0 carries the two real rows
-  // k2 = 0 and k2 = N/2 as A + iB (see half_product)
-  float2 t[M];
-  const bool packed = (u == 0);
+  for (int n = 0; n < M; ++n) t[n] = H2 ? rotate<N, false>(Fc[n], n) : Fc[n];
+}
+
+template <int N>
+MQP_HD MQP_FI void team_p2_pre(int st, int u, int h, const float2* G, const float2* F, float2 (&t)[N / 2]) {
+  if (st == 0) {
+    const float2* Gc = G + u * TeamLayout<N>::GS;
+    if (h) team_p2_fold<N, 1>(Gc, t);
+    else team_p2_fold<N, 0>(Gc, t);
+  } else if (st == 1) {
+    const float2* Fc = F + u * TeamLayout<N>::FS;
+    if (h) team_p2_fload<N, 1>(Fc, t);
+    else team_p2_fload<N, 0>(Fc, t);
+  }
+}
+
+// t = conj(conj(F^) G^) in natural order from F^ (fpos slots of t) and the
+// column's G^ half; column 0 carries the two real rows k2 = 0 and k2 = N/2 as
+// A + iB (see half_product)
+template <int N, int H2>
+MQP_HD MQP_FI void team_p2_product(bool packed, const float2* Gh, float2 (&t)[N / 2]) {
+  constexpr int M = N / 2;
+  float2 p[M];
   if (!packed) {
     mqp_no_hoist();
 #pragma unroll
-    for (int m = 0; m < M; ++m) t[m] = cconj(cmulc(f[fpos<M>(m)], Gc[H2 * M + m]));
+    for (int m = 0; m < M; ++m) p[m] = cconj(cmulc(t[fpos<M>(m)], Gh[m]));
   } else {
     mqp_no_hoist();
 #pragma unroll
     for (int m = 0; m < M; ++m) {
       const int mm = H2 ? M - 1 - m : (M - m) & (M - 1);  // the mirror bin's index in this half
       if (mm < m) continue;
-      const float2 Zk = Gc[H2 * M + m], Zn = cconj(Gc[H2 * M + mm]);
-      const float2 Fk = f[fpos<M>(m)], Fn = cconj(f[fpos<M>(mm)]);
+      const float2 Zk = Gh[m], Zn = cconj(Gh[mm]);
+      const float2 Fk = t[fpos<M>(m)], Fn = cconj(t[fpos<M>(mm)]);
       const float2 A = cscale(cadd(Zk, Zn), 0.5f), B = cscale(cmul_mi(csub(Zk, Zn)), 0.5f);
       const float2 Af = cscale(cadd(Fk, Fn), 0.5f), Bf = cscale(cmul_mi(csub(Fk, Fn)), 0.5f);
       const float2 PA = cmulc(Af, A), PB = cmulc(Bf, B);
-      t[m] = cconj(cadd(PA, cmul_pi(PB)));
-      if (mm != m) t[mm] = cconj(cadd(cconj(PA), cmul_pi(cconj(PB))));
+      p[m] = cconj(cadd(PA, cmul_pi(PB)));
+      if (mm != m) p[mm] = cconj(cadd(cconj(PA), cmul_pi(cconj(PB))));
     }
   }
-  fft_reg<M, false>(t);  // conj of the inverse
+#pragma unroll
+  for (int m = 0; m < M; ++m) t[m] = p[m];
+}
+
+template <int N, int H2>
+MQP_HD MQP_FI void team_p2_store_inverse(float2* Gh, const float2 (&t)[N / 2]) {
+  constexpr int M = N / 2;
 #pragma unroll
   for (int s = 0; s < M; ++s) {
     const float2 A = cconj(t[fpos<M>(s)]);
-    Gc[H2 * M + s] = H2 ? rotate<N, true>(A, s) : A;
+    Gh[s] = H2 ? rotate<N, true>(A, s) : A;
   }
 }
 
-template <int N, int H2, typename Sync>
-MQP_HD MQP_FI void team_phase2(int u, float2* G, const float2* F, Sync sync) {
-  mqp_no_hoist();
-  float2 x[N / 2];
-  team_p2_fold<N, H2>(u, G, x);
-  sync();  // all columns read before the halves are written back
-  team_p2_corr<N, H2>(u, G, F, x);
+template <int N>
+MQP_HD MQP_FI void team_p2_post(int st, int u, int h, float2* G, float2 (&t)[N / 2]) {
+  constexpr int M = N / 2;
+  float2* Gh = G + u * TeamLayout<N>::GS + h * M;
+  if (st == 0) {
+#pragma unroll
+    for (int m = 0; m < M; ++m) Gh[m] = t[fpos<M>(m)];
+  } else if (st == 1) {
+    if (h) team_p2_product<N, 1>(u == 0, Gh, t);
+    else team_p2_product<N, 0>(u == 0, Gh, t);
+  } else {
+    if (h) team_p2_store_inverse<N, 1>(Gh, t);
+    else team_p2_store_inverse<N, 0>(Gh, t);
+  }
+}
+
+// On return G[u] holds A0 in slots 0..M-1 and W_N^-s A1[s] in slots M..N-1.
+template <int N, typename Sync>
+MQP_HD MQP_FI void team_phase2(int u, int h, float2* G, const float2* F, Sync sync) {
+  float2 t[N / 2];
+#pragma unroll 1
+  for (int st = 0; st < 3; ++st) {
+    team_p2_pre<N>(st, u, h, G, F, t);
+    fft_reg<N / 2, false>(t);
+    if (st == 0) sync();
+    team_p2_post<N>(st, u, h, G, t);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -245,8 +299,8 @@ MQP_HD MQP_FI void team_phase2(int u, float2* G, const float2* F, Sync sync) {
 // one decimation-in-frequency step: outputs n = 2j + HH come from a length-M/2
 // FFT of t[k] + t[k+M/2] (HH = 0) or (t[k] - t[k+M/2]) W_M^k (HH = 1).  Output
 // n gives cc[2n] and cc[2n+1]; they go to cc[s1 + P1 * s2] as FP32 (scaled).
-template <int N, int HH>
-MQP_HD MQP_FI void team_phase3_row(int s1, int P1, int P2, const float2* G, float* cc, float scale) {
+template <int N>
+MQP_HD MQP_FI void team_phase3_row(int s1, int hh, int P1, int P2, const float2* G, float* cc, float scale) {
   mqp_no_hoist();
   constexpr int M = N / 2, Q = M / 2, GS = TeamLayout<N>::GS;
   const int s = s1 < M ? s1 : s1 - M;
@@ -262,7 +316,14 @@ MQP_HD MQP_FI void team_phase3_row(int s1, int P1, int P2, const float2* G, floa
     const float2 O = rotate<N, true>(csub(A, B), k);
     return cconj(cadd(E, cmul_pi(O)));
   };
-  auto fold = [](float2 lo, float2 hi, int k) { return HH ? rotate<M, false>(csub(lo, hi), k) : cadd(lo, hi); };
+  // the DIF fold of the half: lo + hi (hh = 0) or (lo - hi) W_M^k (hh = 1),
+  // selected per element so both halves share this code
+  const float fs = hh ? -1.f : 1.f;
+  auto fold = [&](float2 lo, float2 hi, int k) {
+    const float2 d = make_float2(lo.x + fs * hi.x, lo.y + fs * hi.y);
+    const float2 r = rotate<M, false>(d, k);
+    return hh ? r : d;
+  };
   // bins {k, Q-k, Q+k, M-k} close under both pairings (k with M-k for the
   // c2r split, k with k+Q for the DIF fold): four spectrum reads give y[k]
   // and y[Q-k], so only the half-length input stays live
@@ -285,7 +346,7 @@ MQP_HD MQP_FI void team_phase3_row(int s1, int P1, int P2, const float2* G, floa
   fft_reg<Q, false>(y);
 #pragma unroll
   for (int j = 0; j < Q; ++j) {
-    const int n = 2 * j + HH;
+    const int n = 2 * j + hh;
     const float2 T = y[fpos<Q>(j)];
     if (2 * n < P2) cc[s1 + P1 * (2 * n)] = T.x * scale;
     if (2 * n + 1 < P2) cc[s1 + P1 * (2 * n + 1)] = -T.y * scale;

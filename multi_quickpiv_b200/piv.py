@@ -83,8 +83,11 @@ class PIVParameters:
     mask_threshold: float = -1.0
     ndims: int = 3
     ovp_th: float = 0.5
-    # beyond the reference: multi-pass with whole-pixel predictors
-    refine: bool = False
+    # beyond the reference: multi-pass refinement.  False / 0: the reference's
+    # loop (every pass repeats scale 1); True / 1 / "shift": whole-pixel
+    # predictor shifts; 2 / "deform": window deformation around the
+    # interpolated predictor (no masks)
+    refine: object = False
 
     def to_c(self) -> _lib.MqpParams:
         if self.filtFun is not maxval or self.mask_filtFun is not maxval:
@@ -105,8 +108,24 @@ class PIVParameters:
         p.threshold = float(self.threshold)
         p.mask_threshold = float(self.mask_threshold)
         p.ovp_th = float(self.ovp_th)
-        p.refine = int(bool(self.refine))
+        p.refine = refine_code(self.refine)
         return p
+
+
+def refine_code(refine) -> int:
+    """mqp_params.refine for PIVParameters.refine: 0 (False), 1 (True or
+    "shift": whole-pixel predictors) or 2 ("deform": window deformation)."""
+    if isinstance(refine, str):
+        codes = {"none": 0, "shift": 1, "deform": 2}
+        if refine not in codes:
+            raise ValueError(f"refine must be one of {sorted(codes)} or 0, 1, 2")
+        return codes[refine]
+    if isinstance(refine, (bool, np.bool_)):
+        return int(refine)
+    r = int(refine)
+    if r not in (0, 1, 2):
+        raise ValueError("refine must be 0, 1 or 2")
+    return r
 
 
 def setPIVParameters(corr_alg="nsqecc", unpadded=True, good_pad=True, odd_pad=False,
@@ -120,7 +139,7 @@ def setPIVParameters(corr_alg="nsqecc", unpadded=True, good_pad=True, odd_pad=Fa
     return PIVParameters(parseCorr(corr_alg), bool(good_pad), bool(unpadded), bool(odd_pad),
                          toDims3(interSize), toDims3(searchMargin), toDims3(overlap), toDims3(step),
                          int(multipass), bool(computeSN), filtFun, float(threshold), mask_filtFun,
-                         float(mask_threshold), int(ndims), float(ovp_th), bool(refine))
+                         float(mask_threshold), int(ndims), float(ovp_th), refine)
 
 
 def _ovp(p: PIVParameters, scale=1):

@@ -619,9 +619,12 @@ def PIV(img1, img2, p: OracleParams, mask=None, mask_skip=None, refine=False, ke
 
     With ``refine=False`` (the reference's behaviour) every pass of the
     multipass loop re-runs the scale-1 geometry (Q6), so the result equals a
-    single pass.  With ``refine=True`` the build-defined multi-pass runs
-    scales 2^(m-1), ..., 2, 1 with integer predictors taken from the nearest
-    coarser vector (see predictor_from_coarse)."""
+    single pass.  With ``refine=True`` (or 1) the build-defined multi-pass
+    runs scales 2^(m-1), ..., 2, 1 with integer predictors taken from the
+    nearest coarser vector (see predictor_from_coarse); with ``refine=2`` (or
+    "deform") each finer pass runs on the pair deformed around the previous
+    pass's interpolated field (deform_images) and adds that field back at
+    its IA centres."""
     N = np.asarray(img1).ndim
     p.ndims = N
     if not refine or p.multipass <= 1:
@@ -630,14 +633,100 @@ def PIV(img1, img2, p: OracleParams, mask=None, mask_skip=None, refine=False, ke
     size = np.asarray(img1).shape
     pred = None
     prev = None
+    deform = refine in (2, "deform")
+    if deform and mask is not None:
+        raise ValueError("window deformation does not take masks")
     for level in range(p.multipass - 1, -1, -1):
         scale = 2 ** level
-        if prev is not None:
+        a1, a2 = np.asarray(img1), np.asarray(img2)
+        if prev is not None and deform and prev[0].size:
+            # the deforming refinement: the pair resampled around the dense
+            # predictor of the previous pass; this pass measures the residual
+            isz_c, st_c = _isize(p, prev[1]), _step(p, prev[1])
+            a1, a2 = deform_images(a1, a2, prev[0], isz_c, st_c)
+        elif prev is not None and not deform:
             pred = predictor_from_coarse(prev[0], prev[1], size, p, scale)
-        VF, SN = piv_single_pass(img1, img2, p, mask=mask, mask_skip=mask_skip,
+        VF, SN = piv_single_pass(a1, a2, p, mask=mask, mask_skip=mask_skip,
                                  predictor=pred, scale=scale, kappa_out=kappa_out if level == 0 else None)
+        if prev is not None and deform and prev[0].size and VF.size:
+            isz_f, st_f = _isize(p, scale), _step(p, scale)
+            vf = VF.shape[1:]
+            cen = np.stack(np.meshgrid(*[np.arange(n) * st_f[d] + 0.5 * (isz_f[d] - 1)
+                                         for d, n in enumerate(vf)], indexing="ij"), -1)
+            D = deform_predictor(prev[0], _isize(p, prev[1]), _step(p, prev[1]), cen)
+            live = np.ones(vf, dtype=bool)
+            if p.threshold >= 0:
+                for k in np.ndindex(*vf):
+                    sl = tuple(slice(k[d] * st_f[d], k[d] * st_f[d] + isz_f[d]) for d in range(N))
+                    live[k] = not (np.max(a1[sl]) < p.threshold)
+            for d in range(N):
+                VF[d] = np.where(live, VF[d] + D[..., d], VF[d])
         prev = (VF, scale)
     return VF, SN
+
+
+def _deform_weights(f, n):
+    """Clamped multilinear index/weight along one axis: f in fractional index
+    units, n points; returns (j0, j1, t)."""
+    f = np.clip(f, 0.0, float(n - 1))
+    j0 = np.minimum(np.floor(f).astype(np.int64), n - 1)
+    j1 = np.minimum(j0 + 1, n - 1)
+    return j0, j1, f - j0
+
+
+def deform_predictor(VFc, isz_c, st_c, pos):
+    """Build-defined dense predictor (the deforming refinement): the coarse
+    vectors at their IA centres j * step + (interSize - 1) / 2 (0-based),
+    interpolated multilinearly at positions pos (array (..., N)), clamped to
+    the outermost centres; non-finite vectors count as 0.  Weights multiply
+    and terms accumulate in corner order k = 0 .. 2^N - 1 (axis d set when bit
+    d of k is), each product and sum rounded on its own."""
+    N = VFc.shape[0]
+    vf_c = VFc.shape[1:]
+    V = np.where(np.isfinite(VFc), VFc, 0.0)
+    js = [_deform_weights((pos[..., d] - 0.5 * (isz_c[d] - 1)) / st_c[d], vf_c[d]) for d in range(N)]
+    D = np.zeros(pos.shape[:-1] + (N,))
+    for k in range(1 << N):
+        w = np.ones(pos.shape[:-1])
+        idx = []
+        for d in range(N):
+            up = (k >> d) & 1
+            j0, j1, t = js[d]
+            w = w * (t if up else 1.0 - t)
+            idx.append(j1 if up else j0)
+        for c in range(N):
+            D[..., c] = D[..., c] + w * V[(c,) + tuple(idx)]
+    return D
+
+
+def _deform_sample(img, pos):
+    N = img.ndim
+    js = [_deform_weights(pos[..., d], img.shape[d]) for d in range(N)]
+    s = np.zeros(pos.shape[:-1])
+    x = img.astype(np.float64)
+    for k in range(1 << N):
+        w = np.ones(pos.shape[:-1])
+        idx = []
+        for d in range(N):
+            up = (k >> d) & 1
+            j0, j1, t = js[d]
+            w = w * (t if up else 1.0 - t)
+            idx.append(j1 if up else j0)
+        s = s + w * x[tuple(idx)]
+    return s
+
+
+def deform_images(img1, img2, VFc, isz_c, st_c):
+    """The deforming refinement's resampled pair: img1(p - D(p)/2) and
+    img2(p + D(p)/2), multilinear, clamped at the border, in FP64 and then
+    the images' precision."""
+    shape = img1.shape
+    grids = np.meshgrid(*[np.arange(n, dtype=np.float64) for n in shape], indexing="ij")
+    pos = np.stack(grids, -1)
+    D = deform_predictor(VFc, isz_c, st_c, pos)
+    o1 = _deform_sample(img1, pos + (-0.5 * D))
+    o2 = _deform_sample(img2, pos + 0.5 * D)
+    return o1.astype(img1.dtype), o2.astype(img2.dtype)
 
 
 def predictor_from_coarse(VFc, scale_c, size, p, scale_f):

@@ -10,6 +10,7 @@
 
 #include <vector>
 
+#include "mqp_deform.cuh"
 #include "mqp_direct.cuh"
 #include "mqp_piv2d.cuh"
 #include "mqp_piv2d_team.cuh"
@@ -189,9 +190,7 @@ static void emu_team_ia(const Piv2dArgs& a, long long ia, std::vector<float2>& w
   const long long vfo = (long long)v1 + (long long)a.vf1 * v2;
   double vmax = -INFINITY, sumsq = 0.0;
   for (int tid = 0; tid < N; ++tid) {
-    const int hh = tid / M, q = tid % M;
-    if (hh == 0) team_f_row<N, T, ZN, 0>(a, g, sc.meanF, q, F, vmax, sumsq);
-    else team_f_row<N, T, ZN, 1>(a, g, sc.meanF, q, F, vmax, sumsq);
+    team_f_row<N, T, ZN>(a, g, sc.meanF, tid % M, tid / M, F, vmax, sumsq);
   }
   for (int tid = 0; tid < N; ++tid) team_g_row<N, T, ZN>(a, g, (float)sc.meanG, tid, G);
   sc.sumF2 = sumsq;
@@ -203,15 +202,18 @@ static void emu_team_ia(const Piv2dArgs& a, long long ia, std::vector<float2>& w
     return;
   }
   std::vector<float2> xs((size_t)N * M);
-  for (int tid = 0; tid < N; ++tid) {
-    float2(&x)[M] = *reinterpret_cast<float2(*)[M]>(&xs[(size_t)tid * M]);
-    if (tid / M == 0) team_p2_fold<N, 0>(tid % M, G, x);
-    else team_p2_fold<N, 1>(tid % M, G, x);
-  }
-  for (int tid = 0; tid < N; ++tid) {
-    const float2(&x)[M] = *reinterpret_cast<const float2(*)[M]>(&xs[(size_t)tid * M]);
-    if (tid / M == 0) team_p2_corr<N, 0>(tid % M, G, F, x);
-    else team_p2_corr<N, 1>(tid % M, G, F, x);
+  for (int st = 0; st < 3; ++st) {
+    // every thread's transform of the stage, then every thread's post (the
+    // team barrier of stage 0 sits between them)
+    for (int tid = 0; tid < N; ++tid) {
+      float2(&x)[M] = *reinterpret_cast<float2(*)[M]>(&xs[(size_t)tid * M]);
+      team_p2_pre<N>(st, tid % M, tid / M, G, F, x);
+      fft_reg<M, false>(x);
+    }
+    for (int tid = 0; tid < N; ++tid) {
+      float2(&x)[M] = *reinterpret_cast<float2(*)[M]>(&xs[(size_t)tid * M]);
+      team_p2_post<N>(st, tid % M, tid / M, G, x);
+    }
   }
   float* cc = reinterpret_cast<float*>(F);
   const float scale = (float)cc_scale<N>();
@@ -221,8 +223,7 @@ static void emu_team_ia(const Piv2dArgs& a, long long ia, std::vector<float2>& w
     for (int tid = 0; tid < N; ++tid) {
       const int s1 = b + tid % M;
       if (s1 >= paired) continue;
-      if (tid / M == 0) team_phase3_row<N, 0>(s1, P1, P2, G, cc, scale);
-      else team_phase3_row<N, 1>(s1, P1, P2, G, cc, scale);
+      team_phase3_row<N>(s1, tid / M, P1, P2, G, cc, scale);
     }
   if (tail)
     for (int s2 = 0; s2 < P2; ++s2) cc[(P1 - 1) + P1 * s2] = team_tail_value<N>(G, tw, s2) * scale;
@@ -333,6 +334,33 @@ extern "C" __attribute__((visibility("default"))) int mqp_emu_piv2d(
   if (N == 64) return team ? emu_team<64>(a, alg) : (prune ? emu_alg<64, true>(a, alg) : emu_alg<64, false>(a, alg));
   if (N == 32) return team ? emu_team<32>(a, alg) : (prune ? emu_alg<32, true>(a, alg) : emu_alg<32, false>(a, alg));
   return -2;
+}
+
+// the deforming refinement's resampling (mqp_deform.cuh) over a whole image
+extern "C" __attribute__((visibility("default"))) int mqp_emu_deform(
+    const void* img1, const void* img2, int dtype, int nd, const long long* dims, const double* VFc,
+    const int* vf_c, const int* isz_c, const int* st_c, void* out1, void* out2) {
+  DeformArgs a;
+  memset(&a, 0, sizeof(a));
+  a.nd = nd;
+  a.dtype = dtype;
+  long long n = 1;
+  for (int d = 0; d < 3; ++d) {
+    a.dims[d] = d < nd ? dims[d] : 1;
+    n *= a.dims[d];
+    if (d < nd) {
+      a.vf_c[d] = vf_c[d];
+      a.isz_c[d] = isz_c[d];
+      a.st_c[d] = st_c[d];
+    }
+  }
+  a.img1 = img1;
+  a.img2 = img2;
+  a.out1 = out1;
+  a.out2 = out2;
+  a.VFc = VFc;
+  for (long long i = 0; i < n; ++i) deform_pixel(a, i);
+  return 0;
 }
 
 // one register FFT, for direct unit tests of mqp_fft.cuh

@@ -53,3 +53,51 @@ def test_two_pass_3d(alg, gpu):
     VF = _run(i1, i2, alg, (16, 16, 16), (8, 8, 8), (16, 16, 16), 2)
     inner = VF[:, 1:-1, 1:-1, 1:-1]
     assert abs(np.median(inner[0]) - 5.6) < 0.1
+
+
+def _run_deform(i1, i2, alg, IS, SM, st, passes, max_bad_frac=0.0):
+    po = O.set_piv_parameters(corr_alg=alg, interSize=IS, searchMargin=SM, step=st, multipass=passes,
+                              computeSN=True)
+    po.ndims = i1.ndim
+    vf = O.get_vf_size_for(i1.shape, po)
+    kappa = np.full(vf, np.inf)
+    VFo, SNo = O.PIV(i1, i2, po, refine=2, kappa_out=kappa)
+    pp = setPIVParameters(corr_alg=alg, interSize=IS, searchMargin=SM, step=st, multipass=passes, computeSN=True,
+                          refine="deform")
+    VF, SN = PIV(i1, i2, pp)
+    assert VF.shape == VFo.shape
+    bad = (np.abs(VF - VFo) > VF_ATOL).any(axis=0)
+    assert bad.mean() <= max_bad_frac, (np.argwhere(bad)[:5], np.abs(VF - VFo).max())
+    assert (sn_ok(SN, SNo, kappa) | bad).all()
+    return VF
+
+
+@pytest.mark.parametrize("alg", ["fft", "zncc", "nsqecc"])
+def test_deforming_refinement_2d(alg, gpu):
+    """refine = 2: each finer pass runs on the pair deformed around the
+    interpolated coarser field (mqp_deform.cuh), against the oracle's
+    restatement (O.PIV(refine=2))."""
+    i1, i2, _ = synth.pair_2d_vortex(shape=(176, 160), core=40.0, peak=6.0)
+    _run_deform(i1, i2, alg, (16, 16), (4, 4), (8, 8), 2)
+
+
+def test_deforming_refinement_three_passes_float64(gpu):
+    i1, i2, _ = synth.pair_2d_shift(shape=(160, 144), shift=(5.4, -3.3), seed_stream=43)
+    VF = _run_deform(i1, i2, "nsqecc", (8, 8), (4, 4), (8, 8), 3)
+    inner = VF[:, 2:-2, 2:-2]
+    assert abs(np.median(inner[0]) - 5.4) < 0.1 and abs(np.median(inner[1]) + 3.3) < 0.1
+
+
+def test_deforming_refinement_3d(gpu):
+    i1, i2, _ = synth.pair_3d_shear(shape=(64, 64, 64), seed_stream=44, shift=(3.4, -2.1, 1.2), shear=0.02)
+    _run_deform(i1, i2, "fft", (16, 16, 16), (4, 4, 4), (16, 16, 16), 2)
+
+
+def test_deforming_refinement_rejects_masks(gpu):
+    from multi_quickpiv_b200 import _lib
+    i1, i2, _ = synth.pair_2d_shift(shape=(96, 96), seed_stream=45)
+    mask = np.ones_like(i1)
+    pp = setPIVParameters(interSize=(16, 16), searchMargin=(4, 4), step=(16, 16), multipass=2, refine="deform")
+    with pytest.raises(_lib.MQPError) as e:
+        PIV(i1, i2, mask, pp)
+    assert e.value.code == _lib.MQP_ERR_UNSUPPORTED
