@@ -382,6 +382,48 @@ MQP_API int mqp_trajectories(mqp_ctx* ctx, const mqp_traj_params* p, int dtype, 
                              const void* W, float* TY, float* TX, float* TZ);
 
 /*
+ * Time-lapse ingest.  A multi-page TIFF reader (the reference reads its 2D+t
+ * and 3D+t stacks with LIBTIFF, README.md:55-68): classic TIFF in either byte
+ * order, one sample per pixel, strips or tiles, no compression or PackBits,
+ * 8/16/32-bit unsigned or signed integers and 32/64-bit floats.  Pages come
+ * back in Julia's array order: page k of height H and width W is the
+ * column-major H x W array at dst + k*H*W (dimension 1 = image rows).
+ */
+typedef struct mqp_tiff mqp_tiff;
+typedef struct mqp_tiff_info {
+  int64_t width, height, pages;   /* of page 0; pages in the file */
+  int32_t bits, sample_format;    /* BitsPerSample; SampleFormat 1 uint, 2 int, 3 float */
+  int32_t compression, tiled;     /* 1 none, 32773 PackBits; strips (0) or tiles (1) */
+  int32_t uniform;                /* 1 when every page has page 0's size */
+} mqp_tiff_info;
+
+/* Opens (maps) a file; on failure *out may still hold a handle whose
+ * mqp_tiff_last_error says why (close it). */
+MQP_API int mqp_tiff_open(const char* path, mqp_tiff** out);
+MQP_API int mqp_tiff_get_info(const mqp_tiff* t, mqp_tiff_info* info);
+/* Pages [first_page, first_page + npages), all of one size, converted to
+ * dtype (MQP_F32 / MQP_F64) into dst (H*W*npages elements). */
+MQP_API int mqp_tiff_read(mqp_tiff* t, int64_t first_page, int64_t npages, int dtype, void* dst);
+MQP_API const char* mqp_tiff_last_error(const mqp_tiff* t);
+MQP_API int mqp_tiff_close(mqp_tiff* t);
+
+/* A time-lapse frame source over a TIFF stack: frames of pages_per_frame
+ * consecutive pages (1 for 2D+t, the depth for 3D+t), read ahead by a thread
+ * into a ring of `ring` host buffers, pinned when a CUDA device is present
+ * (so their copies to the device run at full speed).  mqp_frame_source_next
+ * blocks until the next frame is read and returns it; the pointer stays
+ * valid until the following call.  MQP_ERR_NOT_FOUND after the last frame
+ * (trailing pages that do not fill a frame are ignored). */
+typedef struct mqp_frame_source mqp_frame_source;
+MQP_API int mqp_frame_source_create(const char* path, int64_t pages_per_frame, int dtype, int ring,
+                                    mqp_frame_source** out);
+/* frames in the stack, a frame's dims (H, W, pages_per_frame), pinned or not */
+MQP_API int mqp_frame_source_info(const mqp_frame_source* s, int64_t* frames, int64_t dims[3], int32_t* pinned);
+MQP_API int mqp_frame_source_next(mqp_frame_source* s, const void** frame, int64_t* index);
+MQP_API const char* mqp_frame_source_last_error(const mqp_frame_source* s);
+MQP_API int mqp_frame_source_destroy(mqp_frame_source* s);
+
+/*
  * Allocation-free 2D PIV.  No counterpart in the reference: it exists for
  * callers that cannot allocate GPU memory when they compute a vector field
  * (code running under a framework that owns all device memory through its

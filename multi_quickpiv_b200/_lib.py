@@ -111,6 +111,12 @@ class MqpPostParams(C.Structure):
     ]
 
 
+class MqpTiffInfo(C.Structure):
+    _fields_ = [("width", C.c_int64), ("height", C.c_int64), ("pages", C.c_int64), ("bits", C.c_int32),
+                ("sample_format", C.c_int32), ("compression", C.c_int32), ("tiled", C.c_int32),
+                ("uniform", C.c_int32)]
+
+
 class MqpTrajParams(C.Structure):
     _fields_ = [
         ("ndims", C.c_int32),
@@ -171,6 +177,16 @@ SIGNATURES = {
                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "mqp_postprocess": (C.c_int, [C.c_void_p, C.POINTER(MqpPostParams), C.POINTER(MqpField), C.c_void_p,
                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "mqp_tiff_open": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
+    "mqp_tiff_get_info": (C.c_int, [C.c_void_p, C.POINTER(MqpTiffInfo)]),
+    "mqp_tiff_read": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_int, C.c_void_p]),
+    "mqp_tiff_last_error": (C.c_char_p, [C.c_void_p]),
+    "mqp_tiff_close": (C.c_int, [C.c_void_p]),
+    "mqp_frame_source_create": (C.c_int, [C.c_char_p, C.c_int64, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "mqp_frame_source_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), I64x3, C.POINTER(C.c_int32)]),
+    "mqp_frame_source_next": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_int64)]),
+    "mqp_frame_source_last_error": (C.c_char_p, [C.c_void_p]),
+    "mqp_frame_source_destroy": (C.c_int, [C.c_void_p]),
     "mqp_traj_count": (C.c_int, [C.POINTER(MqpTrajParams), C.POINTER(C.c_int64)]),
     "mqp_trajectories_device": (C.c_int, [C.c_void_p, C.POINTER(MqpTrajParams), C.c_int, C.c_void_p, C.c_void_p,
                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),

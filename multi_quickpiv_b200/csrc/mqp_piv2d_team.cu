@@ -302,10 +302,11 @@ __global__ void __launch_bounds__(TEAMS * N, MINB)
 
 template <int N>
 struct TeamCfg;
-// length 64: three teams (six warps, ~76 KB) per block, three blocks per SM
+// length 64: two teams (four warps, ~50 KB) per block, four blocks per SM
+// (128 registers); three teams at three blocks (96 registers) spill
 template <>
 struct TeamCfg<64> {
-  static constexpr int TEAMS = 3, MINB = 3;
+  static constexpr int TEAMS = 2, MINB = 4;
 };
 // length 32: eight one-warp teams per block
 template <>
@@ -391,13 +392,15 @@ cudaError_t launch_team_batch_alg(const Piv2dBatch& b, cudaStream_t s, std::stri
 }  // namespace
 
 bool piv2d_team_ok(int N, bool prune, int alg) {
-  // MQP_TUNE_PIV2D_WARP=1 keeps the one-warp-per-IA kernel (for comparisons)
-  static const bool warp_only = [] {
-    const char* v = getenv("MQP_TUNE_PIV2D_WARP");
+  // Opt-in (MQP_TUNE_PIV2D_TEAM=1): on the 2048^2 workload the one-warp-per-IA
+  // kernel is still faster (2.31 ms against 2.51 ms for two 64-thread teams
+  // per block at 128 registers, 2.62 ms for three at 167, 3.58 ms for three
+  // at 96 with spills).
+  static const bool team = [] {
+    const char* v = getenv("MQP_TUNE_PIV2D_TEAM");
     return v && v[0] == '1';
   }();
-  return !warp_only && (N == 32 || N == 64) && prune &&
-         (alg == ALG_FFTCC || alg == ALG_ZNCC || alg == ALG_NSQECC);
+  return team && (N == 32 || N == 64) && prune && (alg == ALG_FFTCC || alg == ALG_ZNCC || alg == ALG_NSQECC);
 }
 
 int piv2d_team_f2(int N, int P1, int P2) {

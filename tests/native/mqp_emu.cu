@@ -327,8 +327,8 @@ extern "C" __attribute__((visibility("default"))) int mqp_emu_piv2d(
   const bool prune = IS1 <= N / 2 && IS2 <= N / 2;
   if (direct2d_ok(IS1, IS2, SM1, SM2)) return emu_piv2d_direct(a, alg);
   if (N == 128) return emu_piv2d_big(a, alg);
-  // as launch_piv2d: pruned FFTCC / ZNCC / NSQECC run on the team kernel
-  // (MQP_EMU_PIV2D_WARP=1 emulates the one-warp-per-IA kernel for them)
+  // the team kernel (launch_piv2d's opt-in variant) for pruned FFTCC / ZNCC /
+  // NSQECC; MQP_EMU_PIV2D_WARP=1 emulates the one-warp-per-IA kernel for them
   const char* warp_env = getenv("MQP_EMU_PIV2D_WARP");
   const bool team = prune && alg <= 2 && !(warp_env && warp_env[0] == '1');
   if (N == 64) return team ? emu_team<64>(a, alg) : (prune ? emu_alg<64, true>(a, alg) : emu_alg<64, false>(a, alg));

@@ -33,7 +33,7 @@ def test_library_exports_every_declared_symbol():
                                       ("mqp_batch_item", "MqpBatchItem"), ("mqp_batch_options", "MqpBatchOptions"),
                                       ("mqp_server_options", "MqpServerOptions"),
                                       ("mqp_server_stats", "MqpServerStats"),
-                                      ("mqp_traj_params", "MqpTrajParams")])
+                                      ("mqp_traj_params", "MqpTrajParams"), ("mqp_tiff_info", "MqpTiffInfo")])
 def test_abi_version_and_struct_layout(tmp_path, cname, py):
     """Each ctypes mirror matches the C layout (size and every field offset),
     checked by compiling a probe against include/mqp.h."""

@@ -192,10 +192,10 @@ def test_emulated_direct_masked(emu):
 @pytest.mark.parametrize("alg", ["fft", "zncc", "nsqecc"])
 @pytest.mark.parametrize("cfg", [((32, 32), (16, 16), (8, 8)), ((16, 16), (8, 8), (8, 8)), ((8, 12), (20, 18), (12, 12))])
 def test_emulated_team_and_warp_kernels_agree(emu, alg, cfg, monkeypatch):
-    """Pruned FFTCC/ZNCC/NSQECC run on the team kernel (one IA per team of N
-    threads); the one-warp-per-IA kernel (MQP_TUNE_PIV2D_WARP=1 on the GPU)
-    stays available.  Both emulations match the oracle and each other within
-    the FP32 plane tolerance."""
+    """Pruned FFTCC/ZNCC/NSQECC run on the one-warp-per-IA kernel or (opt-in,
+    MQP_TUNE_PIV2D_TEAM=1 on the GPU) on the team kernel (one IA per team of
+    N threads).  Both emulations match the oracle and each other within the
+    FP32 plane tolerance."""
     IS, SM, st = cfg
     i1, i2, _ = synth.pair_2d_vortex(shape=(120, 112), seed_stream=27, core=30.0)
     po = O.set_piv_parameters(corr_alg=alg, interSize=IS, searchMargin=SM, step=st, computeSN=True)

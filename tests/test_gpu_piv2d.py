@@ -218,3 +218,29 @@ def test_constant_images_zncc_has_no_peak(gpu):
     VF, SN = PIV(i1, i1, pp)
     assert np.array_equal(VF, VFo) and np.all(VF == -(SM[0] + 1))
     assert np.all(np.isnan(SN)) and np.all(np.isnan(SNo))
+
+
+@pytest.mark.parametrize("alg", ["fft", "zncc", "nsqecc"])
+def test_team_kernel_matches_oracle(alg, gpu):
+    """The opt-in team kernel (one IA per 64-thread team) in a child process
+    with MQP_TUNE_PIV2D_TEAM=1, against the oracle."""
+    import json
+    import os
+    import subprocess
+    import sys
+    code = f"""
+import sys, json, numpy as np
+sys.path.insert(0, {os.path.dirname(os.path.dirname(os.path.abspath(__file__)))!r})
+import oracle.piv_oracle as O
+from multi_quickpiv_b200 import PIV, setPIVParameters, synth
+i1, i2, _ = synth.pair_2d_vortex(shape=(192, 176), core=40.0)
+pp = setPIVParameters(corr_alg={alg!r}, interSize=(32, 32), searchMargin=(16, 16), step=(8, 8), computeSN=True)
+VF, SN = PIV(i1, i2, pp)
+po = O.set_piv_parameters(corr_alg={alg!r}, interSize=(32, 32), searchMargin=(16, 16), step=(8, 8), computeSN=True)
+VFo, SNo = O.PIV(i1, i2, po)
+print(json.dumps({{"err": float(np.max(np.abs(VF - VFo)))}}))
+"""
+    env = dict(os.environ, MQP_TUNE_PIV2D_TEAM="1")
+    r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert json.loads(r.stdout.strip().splitlines()[-1])["err"] <= VF_ATOL

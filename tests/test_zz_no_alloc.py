@@ -90,7 +90,9 @@ def test_noalloc_rejects_images_beyond_its_scratch(gpu):
     p = setPIVParameters(corr_alg="nsqecc", interSize=(32, 32), searchMargin=(16, 16), step=(8, 8))
     p.ndims = 2
     # 4096 x 4096 NSQECC needs one 134 MB integral image: above the built-in scratch
-    rc, msg = _call(lib, p.to_c(), (4096, 4096))
+    import torch
+    vf = torch.zeros(16, dtype=torch.float64, device="cuda")  # never written: the call is rejected first
+    rc, msg = _call(lib, p.to_c(), (4096, 4096), C.c_void_p(vf.data_ptr()))
     assert rc == _lib.MQP_ERR_INVALID and b"scratch" in msg
 
 
