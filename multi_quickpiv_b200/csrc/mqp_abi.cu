@@ -174,13 +174,28 @@ int run_pass_2d(mqp_ctx* ctx, const Problem& pb, const mqp_params* p, const void
                 const int32_t* dpred, double* dplanes, int64_t ia_begin, int64_t ia_end, cudaStream_t s) {
   const int H = (int)pb.dims[0], W = (int)pb.dims[1];
   const int SS1 = pb.IS[0] + 2 * pb.SM[0], SS2 = pb.IS[1] + 2 * pb.SM[1];
-  if (mqp::piv2d_fft_len(SS1, SS2) == 0)
-    return fail(ctx, MQP_ERR_UNSUPPORTED, "2D search window (interSize + 2 searchMargin) above 128 is not supported");
+  const bool huge = mqp::piv2d_fft_len(SS1, SS2) == 0;
+  if (huge && !mqp::piv2d_huge_ok(SS1, SS2, pb.IS[0], pb.IS[1], pb.alg))
+    return fail(ctx, MQP_ERR_UNSUPPORTED,
+                "2D search window (interSize + 2 searchMargin) above 256, or above 128 with an interrogation window "
+                "above 128 or a mask, is not supported");
   if (pb.IS[0] > H || pb.IS[1] > W) return MQP_OK;  // empty vector field
   int rc = integrals_2d(ctx, pb, d1, d2, dtype, s, 0, W);
   if (rc != MQP_OK) return rc;
-  return launch_2d(ctx, args_2d(ctx, pb, p, d1, d2, dmask, dskip, dtype, dVF, dSN, dpred, dplanes, ia_begin, ia_end),
-                   pb.alg, s);
+  mqp::Piv2dArgs a = args_2d(ctx, pb, p, d1, d2, dmask, dskip, dtype, dVF, dSN, dpred, dplanes, ia_begin, ia_end);
+  if (huge) {
+    cudaError_t e = ctx->huge.ensure(mqp::piv2d_huge_scratch_bytes(ctx->device));
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "scratch of the 2D kernel for search windows above 128");
+    a.huge = (float2*)ctx->huge.ptr;
+    std::string err;
+    {
+      ProfileScope ps(ctx, s, 1, ia_end - ia_begin);
+      e = mqp::launch_piv2d_huge(a, pb.alg, s, err);
+    }
+    if (e != cudaSuccess) return fail(ctx, e == cudaErrorInvalidValue ? MQP_ERR_UNSUPPORTED : MQP_ERR_CUDA, err);
+    return MQP_OK;
+  }
+  return launch_2d(ctx, a, pb.alg, s);
 }
 
 size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }

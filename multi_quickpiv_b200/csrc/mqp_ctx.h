@@ -48,6 +48,7 @@ struct mqp_ctx {
   mqp_host::DevBuf img1, img2, mask, mask_skip, II1, IIg, IIg2, VF, SN, pred, planes, status, iscratch, scratch3d;
   mqp_host::DevBuf passVF[2];  // vectors of the coarse passes of a multi-pass refinement
   mqp_host::DevBuf def1, def2;  // deformed images of the deforming refinement
+  mqp_host::DevBuf huge;        // scratch slots of the 2D kernel for search windows above 128
   mqp_host::DevBuf post_in, post_mask, post_out, post_outf, post_mask_out, post_scratch;
   mqp_host::DevBuf traj_in, traj_out;  // host-array pseudo-trajectories
   // host-array 2D path: copy-in and copy-out streams, events of its pieces

@@ -65,6 +65,14 @@ struct Piv2dBatch {
 int piv2d_warp_f2(int N, bool prune, int P1, int P2, bool masked);
 cudaError_t launch_piv2d_batch(const Piv2dBatch& b, cudaStream_t s, std::string& err);
 
+// Search windows of 129..256 (FFT length 256, interrogation windows up to
+// 128, FFTCC / ZNCC / NSQECC): one 256-thread block per IA over a scratch
+// slot per resident block (mqp_piv2d_huge.cu); a.huge must point at
+// piv2d_huge_scratch_bytes(device) bytes.
+bool piv2d_huge_ok(int SS1, int SS2, int IS1, int IS2, int alg);
+size_t piv2d_huge_scratch_bytes(int device);
+cudaError_t launch_piv2d_huge(const Piv2dArgs& a, int alg, cudaStream_t s, std::string& err);
+
 // Team variant of the fused 2D kernel (mqp_piv2d_team.cu): one IA per team
 // of N threads for FFT lengths 32 and 64 with pruned F (interrogation window
 // up to N/2) and FFTCC / ZNCC / NSQECC.  piv2d_team_ok says whether a variant

@@ -57,6 +57,7 @@ struct Piv2dArgs {
   double mask_threshold; // masked: skip when max(mask_skip IA) < mask_threshold (> 0)
   int computeSN;
   int* status;           // device error flag (non-zero = failure), or null
+  float2* huge;          // FFT length 256 (mqp_piv2d_huge.cuh): one scratch slot per resident block
 };
 
 // Geometry of one IA in pad coordinates (0-based).  Pad index p along an

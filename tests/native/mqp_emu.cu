@@ -288,6 +288,7 @@ static int emu_alg(const Piv2dArgs& a, int alg) {
 
 int emu_piv2d_big(const Piv2dArgs& a, int alg);     // mqp_emu_big.cu
 int emu_piv2d_direct(const Piv2dArgs& a, int alg);  // mqp_emu_direct.cu
+int emu_piv2d_huge(const Piv2dArgs& a, int alg);    // mqp_emu_huge.cu
 
 extern "C" __attribute__((visibility("default"))) int mqp_emu_piv2d(
     const void* img1, const void* img2, const void* mask, const void* mask_skip, int dtype, int H, int W,
@@ -323,10 +324,11 @@ extern "C" __attribute__((visibility("default"))) int mqp_emu_piv2d(
   a.threshold = threshold;
   a.computeSN = computeSN;
   const int SS = (IS1 + 2 * SM1) > (IS2 + 2 * SM2) ? (IS1 + 2 * SM1) : (IS2 + 2 * SM2);
-  const int N = SS <= 32 ? 32 : (SS <= 64 ? 64 : (SS <= 128 ? 128 : 0));
+  const int N = SS <= 32 ? 32 : (SS <= 64 ? 64 : (SS <= 128 ? 128 : (SS <= 256 ? 256 : 0)));
   const bool prune = IS1 <= N / 2 && IS2 <= N / 2;
   if (direct2d_ok(IS1, IS2, SM1, SM2)) return emu_piv2d_direct(a, alg);
   if (N == 128) return emu_piv2d_big(a, alg);
+  if (N == 256) return IS1 <= 128 && IS2 <= 128 ? emu_piv2d_huge(a, alg) : -2;
   // the team kernel (launch_piv2d's opt-in variant) for pruned FFTCC / ZNCC /
   // NSQECC; MQP_EMU_PIV2D_WARP=1 emulates the one-warp-per-IA kernel for them
   const char* warp_env = getenv("MQP_EMU_PIV2D_WARP");

@@ -215,3 +215,22 @@ def test_emulated_team_and_warp_kernels_agree(emu, alg, cfg, monkeypatch):
     assert np.array_equal(fin, np.isfinite(out["team"]))  # 0/0 lags (ZNCC in the padding) alike
     scale = np.max(np.abs(out["warp"][fin]))
     assert np.max(np.abs(out["team"][fin] - out["warp"][fin])) <= 2 * PLANE_RTOL * scale
+
+
+@pytest.mark.parametrize("alg", ["fft", "zncc", "nsqecc"])
+@pytest.mark.parametrize("cfg", [((64, 64), (64, 64), (64, 64)), ((128, 128), (32, 32), (96, 96)),
+                                 ((100, 80), (70, 50), (90, 80)), ((128, 128), (64, 64), (128, 128)),
+                                 ((40, 120), (100, 20), (70, 60))])
+def test_emulated_window256_kernel_matches_oracle(emu, alg, cfg):
+    """Search windows of 129..256: one 256-thread block per IA over a scratch slot."""
+    IS, SM, st = cfg
+    i1, i2, _ = synth.pair_2d_vortex(shape=(330, 300), seed_stream=23, core=60.0)
+    po = O.set_piv_parameters(corr_alg=alg, interSize=IS, searchMargin=SM, step=st, computeSN=True)
+    po.ndims = 2
+    VFo, SNo, Co = O.piv_single_pass(i1, i2, po, keep_corr=True)
+    VF, SN, PL = run_emu(emu, i1, i2, alg, IS, SM, st)
+    worst, near_tie = compare_planes(PL, Co, i1.shape, IS, SM, st)
+    assert worst <= PLANE_RTOL, worst
+    bad = (np.abs(VF - VFo) > VF_ATOL).any(axis=0) & ~near_tie
+    assert not bad.any()
+    assert (sn_ok(SN, SNo, sn_condition(Co, i1.shape, IS, SM, st)) | near_tie).all()

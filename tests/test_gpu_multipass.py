@@ -101,3 +101,13 @@ def test_deforming_refinement_rejects_masks(gpu):
     with pytest.raises(_lib.MQPError) as e:
         PIV(i1, i2, mask, pp)
     assert e.value.code == _lib.MQP_ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("alg", ["fft", "zncc"])
+def test_three_pass_2d_from_window256(alg, gpu):
+    """interSize 32 / margin 16 in three passes: the coarsest (interSize 128,
+    margin 64) runs on the search-window-256 kernel."""
+    i1, i2, _ = synth.pair_2d_shift(shape=(416, 384), shift=(27.3, -33.6), seed_stream=42, dtype=np.float32)
+    VF = _run(i1, i2, alg, (32, 32), (16, 16), (32, 32), 3)
+    inner = VF[:, 2:-2, 2:-2]
+    assert abs(np.median(inner[0]) - 27.3) < 0.2 and abs(np.median(inner[1]) + 33.6) < 0.2

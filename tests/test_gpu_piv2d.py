@@ -244,3 +244,34 @@ print(json.dumps({{"err": float(np.max(np.abs(VF - VFo)))}}))
     r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     assert json.loads(r.stdout.strip().splitlines()[-1])["err"] <= VF_ATOL
+
+
+@pytest.mark.parametrize("alg", ["fft", "zncc", "nsqecc"])
+@pytest.mark.parametrize("cfg", [((64, 64), (64, 64), (64, 64)), ((128, 128), (32, 32), (96, 96)),
+                                 ((100, 80), (70, 50), (90, 80)), ((128, 128), (64, 64), (128, 128))],
+                         ids=["is64sm64", "is128sm32", "aniso", "ss256"])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_piv2d_window256_matches_oracle(alg, cfg, dtype, gpu):
+    """Search windows 129..256 run on the 256-thread block kernel."""
+    i1, i2, _ = synth.pair_2d_vortex(shape=(460, 420), seed_stream=26, core=80.0, peak=20.0)
+    _compare(i1.astype(dtype), i2.astype(dtype), alg, *cfg)
+
+
+def test_piv2d_window256_threshold_skip(gpu):
+    i1, i2, _ = synth.pair_2d_shift(shape=(384, 384), shift=(30.2, -41.7), seed_stream=27)
+    i1 = i1.copy()
+    i1[:140, :140] = -5.0
+    VF, VFo = _compare(i1, i2, "fft", (128, 128), (64, 64), (128, 128), thr=0.0)
+    assert np.all(VF[:, 0, 0] == 0)
+
+
+def test_piv2d_window_limits(gpu):
+    from multi_quickpiv_b200 import MQPError, _lib
+    i1, i2, _ = synth.pair_2d_shift(shape=(320, 320))
+    mask = np.ones_like(i1)
+    with pytest.raises(MQPError) as e:  # a mask at a search window above 128
+        PIV(i1, i2, mask, setPIVParameters(interSize=(64, 64), searchMargin=(40, 40), step=(64, 64)))
+    assert e.value.code == _lib.MQP_ERR_UNSUPPORTED
+    with pytest.raises(MQPError) as e:  # above 256
+        PIV(i1, i2, setPIVParameters(interSize=(64, 64), searchMargin=(100, 100), step=(64, 64)))
+    assert e.value.code == _lib.MQP_ERR_UNSUPPORTED
