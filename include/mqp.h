@@ -115,7 +115,12 @@ MQP_API int mqp_vf_dims(const mqp_params* p, int ndims, const int64_t dims[3], i
  * mask != NULL selects masked NSQECC; mask_skip (nullable) is the separate
  * skip mask of the double-masked method (src/multi_quickPIV.jl:27-29).  VF
  * receives N*prod(vf) doubles, SN (nullable; used when computeSN) prod(vf).
- * Blocks until the result is in VF/SN. */
+ * Blocks until the result is in VF/SN.
+ * Window limits (the reference takes any size; beyond these the call
+ * returns MQP_ERR_UNSUPPORTED): 2D search windows interSize + 2 searchMargin
+ * up to 256 per axis, above 128 only unmasked with interrogation windows up
+ * to 128; 3D up to 128 per axis, above 64 with interrogation windows up to
+ * 64.  Refinement passes run at scaled windows and must fit as well. */
 MQP_API int mqp_piv(mqp_ctx* ctx, const void* img1, const void* img2, const void* mask,
             const void* mask_skip, int dtype, int ndims, const int64_t dims[3],
             const mqp_params* p, double* VF, double* SN, int64_t vf_dims_out[3]);

@@ -73,8 +73,7 @@ __device__ __forceinline__ void huge_ia(const Piv2dArgs& a, long long ia, float2
   // ---- A: rows ----
   double vmax = -INFINITY, sumsq = 0.0;
   huge_f_row<T, ZN>(a, g, sc.meanF, t % MH, t / MH, FS, vmax, sumsq);
-  huge_g_row<T, ZN>(a, g, (float)sc.meanG, t, 0, GS, reinterpret_cast<float*>(park));
-  huge_g_row<T, ZN>(a, g, (float)sc.meanG, t, 1, GS, reinterpret_cast<float*>(park));
+  huge_g_row<T, ZN>(a, g, (float)sc.meanG, t, GS, reinterpret_cast<float*>(park));
   vmax = hmax(vmax);
   sumsq = hsum(sumsq);
   if (lane == 0) {

@@ -44,7 +44,8 @@ struct HugeSlot {
 };
 
 // Shared memory (float2 units): the park/exchange area of stage B (64
-// columns x 4 quarters x 64 values), the packed column's staging (2 x 256),
+// columns x 4 quarters x 64 values, element (col, q, m) at m * 256 + q * 64 +
+// col so that a warp's 32 columns fall in distinct banks), the packed column's staging (2 x 256),
 // the twiddle table (256) and reduction slots.
 struct HugeSmem {
   static constexpr int PARK = 64 * 4 * QH;
@@ -77,51 +78,49 @@ MQP_HD MQP_FI void huge_row_bins(const float2 (&w)[QH], float2* out, long long k
   }
 }
 
-// G row t, half hh: data on the clipped search region (minus the search mean
-// for ZNCC), packed z[n] = x[2n] + i x[2n+1], folded z[n] +- z[n+64] (twiddled
-// for hh = 1), transformed, bins of parity hh to GS[k2 * 256 + t].  Each
-// 128-pixel half of the row passes through the thread's column of `stage`
-// (stage[x * 256 + t], 128 KB of shared memory): register-resident loads of a
-// whole row would need an address pair per pixel and spill.
+// G row t: data on the clipped search region (minus the search mean for
+// ZNCC), packed z[n] = x[2n] + i x[2n+1], folded z[n] + z[n+64] (half 0) and
+// (z[n] - z[n+64]) W_128^n (half 1), each transformed and finished into the
+// bins of its parity at GS[k2 * 256 + t].  Every pixel is loaded once: the
+// first 128 pass through the thread's column of `stage` (stage[x * 256 + t],
+// 128 KB of shared memory), the second 128 meet them there, half 0's fold
+// stays in registers and half 1's difference goes back to the stage.
 template <typename T, bool ZNCC>
-MQP_HD MQP_FI void huge_g_row(const Piv2dArgs& a, const IAGeom& g, float mg, int t, int hh, float2* GS,
-                              float* stage) {
-  float2 w[QH];
+MQP_HD MQP_FI void huge_g_row(const Piv2dArgs& a, const IAGeom& g, float mg, int t, float2* GS, float* stage) {
   const bool live = t >= g.lo1 && t < g.hi1;
   const T* src = reinterpret_cast<const T*>(a.img2) + ((long long)(g.g01 + t) + (long long)a.H * g.g02);
   const long long H = a.H;
   float* col = stage + t;
-  auto stage_half = [&](int x0) {
-#pragma unroll 8
-    for (int x = 0; x < MH; ++x) {
-      const int xx = x0 + x;
-      float v = 0.f;
-      if (live && xx >= g.lo2 && xx < g.hi2) {
-        v = (float)ldg_px<T>(src, H * xx);
-        if (ZNCC) v -= mg;
-      }
-      col[x * NH] = v;
+  auto px = [&](int xx) {
+    float v = 0.f;
+    if (live && xx >= g.lo2 && xx < g.hi2) {
+      v = (float)ldg_px<T>(src, H * xx);
+      if (ZNCC) v -= mg;
     }
+    return v;
   };
-  stage_half(0);
-#pragma unroll
-  for (int n = 0; n < QH; ++n) w[n] = make_float2(col[(2 * n) * NH], col[(2 * n + 1) * NH]);
-  mqp_no_hoist();
-  stage_half(MH);
-  const float fs = hh ? -1.f : 1.f;
+#pragma unroll 16
+  for (int x = 0; x < MH; ++x) col[x * NH] = px(x);
+  float2 w[QH];
 #pragma unroll
   for (int n = 0; n < QH; ++n) {
-    const float2 hi = make_float2(col[(2 * n) * NH], col[(2 * n + 1) * NH]);
-    w[n] = make_float2(w[n].x + fs * hi.x, w[n].y + fs * hi.y);
-  }
-  if (hh) {
-#pragma unroll
-    for (int n = 1; n < QH; ++n) w[n] = rotate<MH, false>(w[n], n);
+    if (n % 8 == 0) mqp_no_hoist();
+    const float h0 = px(MH + 2 * n), h1 = px(MH + 2 * n + 1);
+    const float l0 = col[(2 * n) * NH], l1 = col[(2 * n + 1) * NH];
+    w[n] = make_float2(l0 + h0, l1 + h1);
+    col[(2 * n) * NH] = l0 - h0;
+    col[(2 * n + 1) * NH] = l1 - h1;
   }
   fft_reg<QH, false>(w);
-  float2* out = GS + t;
-  if (hh) huge_row_bins<1>(w, out, NH);
-  else huge_row_bins<0>(w, out, NH);
+  huge_row_bins<0>(w, GS + t, NH);
+  mqp_no_hoist();
+#pragma unroll
+  for (int n = 0; n < QH; ++n) {
+    const float2 d = make_float2(col[(2 * n) * NH], col[(2 * n + 1) * NH]);
+    w[n] = n ? rotate<MH, false>(d, n) : d;
+  }
+  fft_reg<QH, false>(w);
+  huge_row_bins<1>(w, GS + t, NH);
 }
 
 // F row q (< 128), half hh: the IA row (minus the IA mean for ZNCC), at most
@@ -190,8 +189,11 @@ MQP_HD MQP_FI void huge_fold4(int q, Src src, const float2* tw, float2 (&y)[QH])
   }
 }
 
+// Element stride of one thread's park slots (see HugeSmem).
+constexpr int HPS = 4 * 64;
+
 // Part 1 of a column: G's quarter transformed and parked in shared memory
-// (park[m] = G^[4m + q], natural m) and F's quarter transformed into f.
+// (park[m * HPS] = G^[4m + q], natural m) and F's quarter transformed into f.
 MQP_HD MQP_FI void huge_col_forward(int k2, int q, const float2* GS, const float2* FS, const float2* tw,
                                     float2* park, float2 (&f)[QH]) {
   mqp_no_hoist();
@@ -201,7 +203,7 @@ MQP_HD MQP_FI void huge_col_forward(int k2, int q, const float2* GS, const float
     huge_fold4(q, [&](int j, int n) { return gc[n + QH * j]; }, tw, y);
     fft_reg<QH, false>(y);
 #pragma unroll
-    for (int m = 0; m < QH; ++m) park[m] = y[fpos<QH>(m)];
+    for (int m = 0; m < QH; ++m) park[m * HPS] = y[fpos<QH>(m)];
   }
   mqp_no_hoist();
   const float2* fc = FS + (long long)k2 * MH;
@@ -211,14 +213,14 @@ MQP_HD MQP_FI void huge_col_forward(int k2, int q, const float2* GS, const float
 }
 
 // Part 2: t = conj(conj(F^) G^) for the quarter's bins, written over the
-// park (park[m] for bin 4m + q) so that f dies before the inverse loads it.
+// park (park[m * HPS] for bin 4m + q) so that f dies before the inverse loads it.
 // The packed column k2 = 0 carries the real rows k2 = 0 and 128 as A + iB;
 // its product pairs bin k with -k, whose quarter is (-q) mod 4, so the quad
 // stages both spectra in `pack` (G^ then F^, natural bin order) first.
 MQP_HD MQP_FI void huge_col_product(int k2, int q, float2* park, const float2* pack, const float2 (&f)[QH]) {
   if (k2 != 0) {
 #pragma unroll
-    for (int m = 0; m < QH; ++m) park[m] = cconj(cmulc(f[fpos<QH>(m)], park[m]));
+    for (int m = 0; m < QH; ++m) park[m * HPS] = cconj(cmulc(f[fpos<QH>(m)], park[m * HPS]));
     return;
   }
   const float2* Gp = pack;
@@ -230,36 +232,37 @@ MQP_HD MQP_FI void huge_col_product(int k2, int q, float2* park, const float2* p
     const float2 A = cscale(cadd(Zk, Zn), 0.5f), B = cscale(cmul_mi(csub(Zk, Zn)), 0.5f);
     const float2 Af = cscale(cadd(Fk, Fn), 0.5f), Bf = cscale(cmul_mi(csub(Fk, Fn)), 0.5f);
     const float2 PA = cmulc(Af, A), PB = cmulc(Bf, B);
-    park[m] = cconj(cadd(PA, cmul_pi(PB)));
+    park[m * HPS] = cconj(cadd(PA, cmul_pi(PB)));
   }
 }
 
 // Part 3: the quarter's 64-point inverse (through the forward transform of
-// the conjugate products parked at park[m]), twiddled W_256^{-s q} z_q[s],
-// written back over the park: park[s] = xch[q][s] of the quad's area.
+// the conjugate products parked at park[m * HPS]), twiddled W_256^{-s q}
+// z_q[s], written back over the park: park[s * HPS] = xch[q][s].
 MQP_HD MQP_FI void huge_col_inverse(int q, float2* park, const float2* tw) {
   mqp_no_hoist();
   float2 t[QH];
 #pragma unroll
-  for (int m = 0; m < QH; ++m) t[m] = park[m];
+  for (int m = 0; m < QH; ++m) t[m] = park[m * HPS];
   fft_reg<QH, false>(t);
 #pragma unroll
   for (int s = 0; s < QH; ++s) {
     const float2 z = cconj(t[fpos<QH>(s)]);
     const float2 w = tw[(s * q) & (NH - 1)];  // W_256^{-sq} = cos + i sin
-    park[s] = make_float2(z.x * w.x - z.y * w.y, z.x * w.y + z.y * w.x);
+    park[s * HPS] = make_float2(z.x * w.x - z.y * w.y, z.x * w.y + z.y * w.x);
   }
 }
 
 // Part 4 (after the quad's exchange): lags s1 = s + 64 p of the column,
-//   x[s + 64p] = sum_q W_4^{-pq} xch[q][s],
+//   x[s + 64p] = sum_q W_4^{-pq} xch[q][s],   xch[q][s] = xch[s * HPS + q * 64],
 // those below P1 to LG[k2 * 256 + s1].
 MQP_HD MQP_FI void huge_col_combine(int k2, int p, int P1, const float2* xch, float2* LG) {
 #pragma unroll 4
   for (int s = 0; s < QH; ++s) {
     const int s1 = s + QH * p;
     if (s1 >= P1) break;
-    const float2 a0 = xch[s], a1 = xch[QH + s], a2 = xch[2 * QH + s], a3 = xch[3 * QH + s];
+    const float2* e = xch + s * HPS;
+    const float2 a0 = e[0], a1 = e[QH], a2 = e[2 * QH], a3 = e[3 * QH];
     float2 v;
     // W_4^{-pq} = (+i)^{pq}
     if (p == 0) v = cadd(cadd(a0, a1), cadd(a2, a3));
@@ -273,18 +276,18 @@ MQP_HD MQP_FI void huge_col_combine(int k2, int p, int P1, const float2* xch, fl
 // Stage B for thread t in round r (columns k2 = 64 r + t % 64, quarter
 // q = t / 64): part 1, then (block barrier) part 2, then (block barrier)
 // part 3, then a block barrier before the next round reuses the park.
-// park: 64 columns x 4 quarters x 64 values; the quad of column c exchanges
-// through park[c * 256 ...].
+// park: 64 columns x 4 quarters x 64 values (HugeSmem); the quad of column c
+// exchanges through its own slots, based at park[c].
 MQP_HD MQP_FI void huge_b_part1(int r, int t, const float2* GS, const float2* FS, const float2* tw, float2* park,
                                 float2* pack, float2 (&f)[QH]) {
   const int col = t % 64, q = t / 64, k2 = r * 64 + col;
-  float2* mine = park + (col * 4 + q) * QH;
+  float2* mine = park + q * 64 + col;
   huge_col_forward(k2, q, GS, FS, tw, mine, f);
   if (k2 == 0) {
     // the packed column's spectra in natural bin order for its mirror pairs
 #pragma unroll
     for (int m = 0; m < QH; ++m) {
-      pack[4 * m + q] = mine[m];
+      pack[4 * m + q] = mine[m * HPS];
       pack[NH + 4 * m + q] = f[fpos<QH>(m)];
     }
   }
@@ -292,13 +295,13 @@ MQP_HD MQP_FI void huge_b_part1(int r, int t, const float2* GS, const float2* FS
 MQP_HD MQP_FI void huge_b_part2(int r, int t, const float2* tw, float2* park, const float2* pack,
                                 const float2 (&f)[QH]) {
   const int col = t % 64, q = t / 64, k2 = r * 64 + col;
-  float2* mine = park + (col * 4 + q) * QH;
+  float2* mine = park + q * 64 + col;
   huge_col_product(k2, q, mine, pack, f);
   huge_col_inverse(q, mine, tw);
 }
 MQP_HD MQP_FI void huge_b_part3(int r, int t, int P1, const float2* park, float2* LG) {
   const int col = t % 64, q = t / 64, k2 = r * 64 + col;
-  huge_col_combine(k2, q, P1, park + col * 4 * QH, LG);
+  huge_col_combine(k2, q, P1, park + col, LG);
 }
 
 // ---------------------------------------------------------------------------

@@ -40,8 +40,7 @@ static void emu_huge_ia(const Piv2dArgs& a, long long ia, float2* slot, float2* 
   double vmax = -INFINITY, sumsq = 0.0;
   for (int t = 0; t < HUGE_THREADS; ++t) {
     huge_f_row<T, ZN>(a, g, sc.meanF, t % MH, t / MH, FS, vmax, sumsq);
-    huge_g_row<T, ZN>(a, g, (float)sc.meanG, t, 0, GS, reinterpret_cast<float*>(park));
-    huge_g_row<T, ZN>(a, g, (float)sc.meanG, t, 1, GS, reinterpret_cast<float*>(park));
+    huge_g_row<T, ZN>(a, g, (float)sc.meanG, t, GS, reinterpret_cast<float*>(park));
   }
   sc.sumF2 = sumsq;
   if (a.threshold >= 0.0 && vmax < a.threshold) {
