@@ -100,7 +100,7 @@ static int integrals_2d(mqp_ctx* ctx, const Problem& pb, const void* d1, const v
     return whole ? mqp::launch_integral2d(img, dtype, H, W, sq, out, isc, s)
                  : mqp::launch_integral2d_cols(img, dtype, H, W, x0, x1, sq, out, isc, s);
   };
-  {
+  if (!mqp::piv2d_local_sums(pb.IS[0], pb.IS[1], pb.SM[0], pb.SM[1], pb.alg)) {
     ProfileScope ps(ctx, s, 0, 0);
     if ((e = ctx->IIg2.ensure(ii_bytes)) != cudaSuccess) return cuda_fail(ctx, e, "integral buffer");
     if ((e = integral(d2, true, (double*)ctx->IIg2.ptr, 0)) != cudaSuccess)

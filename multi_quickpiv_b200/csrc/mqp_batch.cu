@@ -241,6 +241,7 @@ int mqp_batch_plan_create(mqp_ctx* ctx, const mqp_batch_item* items, int32_t n_i
     int N = 0;
     bool prune = false;
     int alg = 0, dtype = 0;
+    bool lw = false;  // window sums on chip (piv2d_local_sums), as the single-pair path
     int wf2 = 0;
     std::vector<int> members;
     size_t items_off = 0, prefix_off = 0, counter_off = 0;
@@ -249,7 +250,7 @@ int mqp_batch_plan_create(mqp_ctx* ctx, const mqp_batch_item* items, int32_t n_i
   };
   std::vector<std::vector<Group>> groups(rounds);
   for (int r = 0; r < rounds; ++r) {
-    std::map<std::tuple<int, int, int, int>, int> idx;
+    std::map<std::tuple<int, int, int, int, int>, int> idx;
     for (int k = 0; k < n_items; ++k) {
       const ItemPlan& ip = plan[k];
       const int l = ip.levels - 1 - r;
@@ -260,7 +261,8 @@ int mqp_batch_plan_create(mqp_ctx* ctx, const mqp_batch_item* items, int32_t n_i
       const bool direct = mqp::direct2d_ok(pb.IS[0], pb.IS[1], pb.SM[0], pb.SM[1]);
       const int N = direct ? 1 : mqp::piv2d_fft_len(pb.IS[0] + 2 * pb.SM[0], pb.IS[1] + 2 * pb.SM[1]);
       const bool prune = direct || (pb.IS[0] <= N / 2 && pb.IS[1] <= N / 2);
-      const auto key = std::make_tuple(N, (int)prune, ip.alg, (int)ip.it.dtype);
+      const bool lw = !direct && mqp::piv2d_local_sums(pb.IS[0], pb.IS[1], pb.SM[0], pb.SM[1], ip.alg);
+      const auto key = std::make_tuple(N, (int)prune, ip.alg, (int)ip.it.dtype, (int)lw);
       auto f = idx.find(key);
       if (f == idx.end()) {
         Group g;
@@ -268,6 +270,7 @@ int mqp_batch_plan_create(mqp_ctx* ctx, const mqp_batch_item* items, int32_t n_i
         g.prune = prune;
         g.alg = ip.alg;
         g.dtype = ip.it.dtype;
+        g.lw = lw;
         idx[key] = (int)groups[r].size();
         groups[r].push_back(g);
         f = idx.find(key);
@@ -275,6 +278,7 @@ int mqp_batch_plan_create(mqp_ctx* ctx, const mqp_batch_item* items, int32_t n_i
       Group& g = groups[r][f->second];
       g.members.push_back(k);
       g.wf2 = std::max(g.wf2, direct ? (mqp::piv2d_direct_words(pb.IS[0], pb.IS[1], pb.SM[0], pb.SM[1]) + 1) / 2
+                              : lw   ? mqp::piv2d_warp_f2_lw(N, 2 * pb.SM[0] + 1, 2 * pb.SM[1] + 1)
                                      : mqp::piv2d_warp_f2(N, prune, 2 * pb.SM[0] + 1, 2 * pb.SM[1] + 1,
                                                           ip.alg == mqp::ALG_MASK_NSQECC));
     }
@@ -485,6 +489,7 @@ int mqp_batch_plan_create(mqp_ctx* ctx, const mqp_batch_item* items, int32_t n_i
       b.dtype = g.dtype;
       b.wf2 = g.wf2;
       b.grab = o.grab;
+      b.lw = g.lw;
       b.counter = at<unsigned long long>(P, g.counter_off);
       P->launches += 1;
       P->ops.push_back([=](cudaStream_t m, const cudaStream_t*) {

@@ -25,6 +25,15 @@
 
 namespace mqp {
 
+// An empty asm statement with a memory clobber: memory operations cannot
+// move across it (loads before it are issued before it, loads after it stay
+// after it).
+MQP_HD MQP_FI void mqp_no_hoist() {
+#if defined(__CUDA_ARCH__)
+  asm volatile("" ::: "memory");
+#endif
+}
+
 constexpr int TW_N = 256;  // twiddle table resolution: exp(2*pi*i*m/256)
 
 // {cos, sin}(2*pi*m/256).  Each translation unit gets its own 2 KB copy

@@ -61,8 +61,10 @@ struct Piv2dBatch {
   int wf2;
   int grab;
   unsigned long long* counter;
+  bool lw;  // every item forms its window sums on chip (piv2d_local_sums)
 };
 int piv2d_warp_f2(int N, bool prune, int P1, int P2, bool masked);
+int piv2d_warp_f2_lw(int N, int P1, int P2);
 cudaError_t launch_piv2d_batch(const Piv2dBatch& b, cudaStream_t s, std::string& err);
 
 // Search windows of 129..256 (FFT length 256, interrogation windows up to
@@ -70,6 +72,9 @@ cudaError_t launch_piv2d_batch(const Piv2dBatch& b, cudaStream_t s, std::string&
 // slot per resident block (mqp_piv2d_huge.cu); a.huge must point at
 // piv2d_huge_scratch_bytes(device) bytes.
 bool piv2d_huge_ok(int SS1, int SS2, int IS1, int IS2, int alg);
+// ZNCC passes whose kernel forms the window sums on chip: they need no
+// integral image of img2^2 (mqp_piv2d.cu).
+bool piv2d_local_sums(int IS1, int IS2, int SM1, int SM2, int alg);
 size_t piv2d_huge_scratch_bytes(int device);
 cudaError_t launch_piv2d_huge(const Piv2dArgs& a, int alg, cudaStream_t s, std::string& err);
 

@@ -252,14 +252,18 @@ __device__ __forceinline__ void warp_peak(double& best, int& bidx) {
 // ---------------------------------------------------------------------------
 // One interrogation area, the whole per-IA body of PIV_CPU's loop, for one
 // warp.  GH is the warp's shared-memory workspace (Layout2d, sized for this
-// IA's lag plane), tw the (cos, sin)(2 pi j / N) table.
-template <int N, bool FPRUNE, int ALG, typename T>
+// IA's lag plane), tw the (cos, sin)(2 pi j / N) table.  LW: ZNCC with an
+// N/2 x N/2 interrogation window forms its window sums on chip (lw_rows /
+// lw_cols) instead of reading integral images.
+template <int N, bool FPRUNE, int ALG, typename T, bool LW = false>
 __device__ __forceinline__ void piv2d_ia(const Piv2dArgs& a, long long ia, float2* GH, const float2* tw, int lane) {
   using Lay = Layout2d<N, FPRUNE>;
   constexpr int M = N / 2;
   constexpr bool MASKED = ALG == ALG_MASK_NSQECC;
+  static_assert(!LW || ((ALG == ALG_ZNCC || ALG == ALG_NSQECC) && FPRUNE), "on-chip window sums: ZNCC / NSQECC");
   const int P1 = 2 * a.SM1 + 1, P2 = 2 * a.SM2 + 1;
-  float2* FH = GH + Lay::F_OFF;
+  float2* FH = GH + (LW ? Lay::F_OFF_LW : Lay::F_OFF);
+  double* lw = LW ? reinterpret_cast<double*>(GH) : nullptr;
   double* plane = reinterpret_cast<double*>(FH);
   float* c1buf = MASKED ? reinterpret_cast<float*>(FH + Lay::region2_f2(P1, P2)) : nullptr;
   const double scale = cc_scale<N>();
@@ -378,6 +382,14 @@ __device__ __forceinline__ void piv2d_ia(const Piv2dArgs& a, long long ia, float
       for (int s2 = lane; s2 < P2; s2 += 32)
         plane[s1 * P2 + s2] = (double)tail_row_value<N, FPRUNE>(GH, tw, s1, s2) * scale;
     __syncwarp();
+    if (LW) {
+      // the G spectra are dead: their space takes the window-sum table
+      lw_rows<N, T, ALG == ALG_ZNCC>(a, g, sc.meanG, lane, P2, lw);
+      __syncwarp();
+      lw_cols<N>(lane, P1, P2, lw);
+      lw_col32<N>(lane, P1, P2, lw);
+      __syncwarp();
+    }
     if (MASKED && pass == 0) {
       // park (F*mask)*G while the second pass reuses the workspace
       for (int i = lane; i < P1 * P2; i += 32) c1buf[i] = (float)plane[i];
@@ -413,12 +425,13 @@ __device__ __forceinline__ void piv2d_ia(const Piv2dArgs& a, long long ia, float
   acc.ssum = 0.0;
 #pragma unroll 1
   for (int s1 = lane; s1 < lane_rows; s1 += 32)
-    finish_row<ALG>(a, g, sc, s1, P1, P2, plane + s1 * P2, R, acc, MASKED ? c1buf + s1 * P2 : nullptr);
+    finish_row<ALG, LW ? N : 0>(a, g, sc, s1, P1, P2, plane + s1 * P2, R, acc, MASKED ? c1buf + s1 * P2 : nullptr,
+                                lw);
 #pragma unroll 1
   for (int s1 = lane_rows; s1 < P1; ++s1)
     for (int s2 = lane; s2 < P2; s2 += 32) {
       double& e = plane[s1 * P2 + s2];
-      e = finish_one<ALG>(a, g, sc, s1, s2, e, MASKED ? (double)c1buf[s1 * P2 + s2] : 0.0);
+      e = finish_one<ALG, LW ? N : 0>(a, g, sc, s1, s2, e, MASKED ? (double)c1buf[s1 * P2 + s2] : 0.0, lw);
       acc_take(acc, R, s1, s2, P1, e);
     }
   __syncwarp();
@@ -450,21 +463,21 @@ __device__ __forceinline__ void piv2d_ia(const Piv2dArgs& a, long long ia, float
 // Persistent: each warp walks IAs ia = first + k * (all warps).  The warp's
 // shared-memory workspace holds the spectra rows of G (N/2 x (N+1)) and F
 // (N/2 x (NF+1)); after phase 2 the F rows are reused for the FP64 plane.
-template <int N, bool FPRUNE, int ALG, typename T, int WARPS, int MINB>
+template <int N, bool FPRUNE, int ALG, typename T, int WARPS, int MINB, bool LW = false>
 __global__ void __launch_bounds__(WARPS * 32, MINB) piv2d_kernel(Piv2dArgs a) {
   extern __shared__ float2 smem[];
   using Lay = Layout2d<N, FPRUNE>;
   constexpr bool MASKED = ALG == ALG_MASK_NSQECC;
   const int P1 = 2 * a.SM1 + 1, P2 = 2 * a.SM2 + 1;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int wf2 = Lay::warp_f2(P1, P2, MASKED);
+  const int wf2 = LW ? Lay::warp_f2_lw(P1, P2) : Lay::warp_f2(P1, P2, MASKED);
   float2* GH = smem + (size_t)warp * wf2;
   float2* tw = smem + (size_t)WARPS * wf2;  // (cos, sin)(2 pi j / N)
   for (int j = threadIdx.x; j < N; j += blockDim.x) tw[j] = twiddle_rt(j * (TW_N / N));
   __syncthreads();
   const long long nwarps = (long long)gridDim.x * WARPS;
   for (long long ia = a.ia_begin + (long long)blockIdx.x * WARPS + warp; ia < a.ia_end; ia += nwarps)
-    piv2d_ia<N, FPRUNE, ALG, T>(a, ia, GH, tw, lane);
+    piv2d_ia<N, FPRUNE, ALG, T, LW>(a, ia, GH, tw, lane);
 }
 
 // Batched: the IAs of many image pairs sharing one kernel variant form one
@@ -472,7 +485,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) piv2d_kernel(Piv2dArgs a) {
 // (prefix[n_items] = total).  Warps take `grab` consecutive queue entries at
 // a time from `counter` (zeroed before the launch), so large and small pairs
 // balance across the SMs.  wf2: float2 per warp, the largest any item needs.
-template <int N, bool FPRUNE, int ALG, typename T, int WARPS, int MINB>
+template <int N, bool FPRUNE, int ALG, typename T, int WARPS, int MINB, bool LW = false>
 __global__ void __launch_bounds__(WARPS * 32, MINB)
     piv2d_batch_kernel(const Piv2dArgs* __restrict__ items, const long long* __restrict__ prefix, int n_items,
                        long long total, int wf2, int grab, unsigned long long* counter) {
@@ -497,7 +510,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
         else hi = mid - 1;
       }
       const Piv2dArgs& a = items[lo];
-      piv2d_ia<N, FPRUNE, ALG, T>(a, a.ia_begin + (gi - prefix[lo]), GH, tw, lane);
+      piv2d_ia<N, FPRUNE, ALG, T, LW>(a, a.ia_begin + (gi - prefix[lo]), GH, tw, lane);
     }
   }
 }
@@ -519,12 +532,13 @@ int device_sm_count(int device) {
   return n;
 }
 
-template <int N, bool FPRUNE, int ALG, typename T, int WARPS, int MINB>
+template <int N, bool FPRUNE, int ALG, typename T, int WARPS, int MINB, bool LW = false>
 static cudaError_t launch_t(const Piv2dArgs& a, cudaStream_t s, std::string& err) {
   using Lay = Layout2d<N, FPRUNE>;
   const int P1 = 2 * a.SM1 + 1, P2 = 2 * a.SM2 + 1;
-  const size_t smem = ((size_t)WARPS * Lay::warp_f2(P1, P2, ALG == ALG_MASK_NSQECC) + N) * sizeof(float2);
-  auto kern = piv2d_kernel<N, FPRUNE, ALG, T, WARPS, MINB>;
+  const int wf2 = LW ? Lay::warp_f2_lw(P1, P2) : Lay::warp_f2(P1, P2, ALG == ALG_MASK_NSQECC);
+  const size_t smem = ((size_t)WARPS * wf2 + N) * sizeof(float2);
+  auto kern = piv2d_kernel<N, FPRUNE, ALG, T, WARPS, MINB, LW>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) {
     err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e);
@@ -567,6 +581,36 @@ static cudaError_t launch_dt(const Piv2dArgs& a, int alg, cudaStream_t s, std::s
                       : launch_alg<N, FPRUNE, double, WARPS, MINB>(a, alg, s, err);
 }
 
+// ZNCC whose interrogation window is half the FFT length in both axes: the
+// warp kernel forms the window sums on chip and reads no integral image of
+// img2^2 (lw_rows / lw_cols).  Measured on B200 (2048^2 vortex, interSize 32,
+// margin 16, step 8, whole pass): ZNCC 2.91 -> 2.77 ms, since it drops eight
+// integral-image loads per lag; NSQECC, with four, ran 2.42 -> 2.54 ms (the
+// window's second read from L2 costs more than the lookups it replaces), so
+// NSQECC keeps the integral image.
+bool piv2d_local_sums(int IS1, int IS2, int SM1, int SM2, int alg) {
+  if (alg != ALG_ZNCC) return false;
+  if (direct2d_ok(IS1, IS2, SM1, SM2)) return false;
+  const int N = piv2d_fft_len(IS1 + 2 * SM1, IS2 + 2 * SM2);
+  if (N != 32 && N != 64) return false;
+  if (piv2d_team_ok(N, true, alg)) return false;
+  return IS1 == N / 2 && IS2 == N / 2;
+}
+
+template <int N, int MINB>
+static cudaError_t launch_lw(const Piv2dArgs& a, int alg, cudaStream_t s, std::string& err) {
+  if (alg != ALG_ZNCC) {
+    err = "on-chip window sums are built for ZNCC";
+    return cudaErrorInvalidValue;
+  }
+  return a.dtype == 0 ? launch_t<N, true, ALG_ZNCC, float, 4, MINB, true>(a, s, err)
+                      : launch_t<N, true, ALG_ZNCC, double, 4, MINB, true>(a, s, err);
+}
+
+int piv2d_warp_f2_lw(int N, int P1, int P2) {
+  return N == 64 ? Layout2d<64, true>::warp_f2_lw(P1, P2) : Layout2d<32, true>::warp_f2_lw(P1, P2);
+}
+
 int piv2d_warp_f2(int N, bool prune, int P1, int P2, bool masked) {
   if (!masked && piv2d_team_ok(N, prune, ALG_NSQECC)) return piv2d_team_f2(N, P1, P2);
   if (N == 128) return piv2d_big_warp_f2(prune, P1, P2, masked);
@@ -575,10 +619,10 @@ int piv2d_warp_f2(int N, bool prune, int P1, int P2, bool masked) {
   return 0;
 }
 
-template <int N, bool FPRUNE, int ALG, typename T, int WARPS, int MINB>
+template <int N, bool FPRUNE, int ALG, typename T, int WARPS, int MINB, bool LW = false>
 static cudaError_t launch_batch_t(const Piv2dBatch& b, cudaStream_t s, std::string& err) {
   const size_t smem = ((size_t)WARPS * b.wf2 + N) * sizeof(float2);
-  auto kern = piv2d_batch_kernel<N, FPRUNE, ALG, T, WARPS, MINB>;
+  auto kern = piv2d_batch_kernel<N, FPRUNE, ALG, T, WARPS, MINB, LW>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) {
     err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e);
@@ -618,6 +662,16 @@ static cudaError_t launch_batch_alg(const Piv2dBatch& b, cudaStream_t s, std::st
   }
 }
 
+template <int N, int MINB>
+static cudaError_t launch_batch_lw(const Piv2dBatch& b, cudaStream_t s, std::string& err) {
+  if (b.alg != ALG_ZNCC) {
+    err = "on-chip window sums are built for ZNCC";
+    return cudaErrorInvalidValue;
+  }
+  return b.dtype == 0 ? launch_batch_t<N, true, ALG_ZNCC, float, 4, MINB, true>(b, s, err)
+                      : launch_batch_t<N, true, ALG_ZNCC, double, 4, MINB, true>(b, s, err);
+}
+
 template <int N, bool FPRUNE>
 static cudaError_t launch_batch_dt(const Piv2dBatch& b, cudaStream_t s, std::string& err) {
   return b.dtype == 0 ? launch_batch_alg<N, FPRUNE, float>(b, s, err) : launch_batch_alg<N, FPRUNE, double>(b, s, err);
@@ -628,6 +682,7 @@ cudaError_t launch_piv2d_batch(const Piv2dBatch& b, cudaStream_t s, std::string&
   if (b.N == 128) return launch_piv2d_big_batch(b, s, err);
   if (b.N == 1) return launch_piv2d_direct_batch(b, s, err);
   if (piv2d_team_ok(b.N, b.prune, b.alg)) return launch_piv2d_team_batch(b, s, err);
+  if (b.lw) return b.N == 64 ? launch_batch_lw<64, 2>(b, s, err) : launch_batch_lw<32, 3>(b, s, err);
   if (b.N == 64) return b.prune ? launch_batch_dt<64, true>(b, s, err) : launch_batch_dt<64, false>(b, s, err);
   if (b.N == 32) return b.prune ? launch_batch_dt<32, true>(b, s, err) : launch_batch_dt<32, false>(b, s, err);
   err = "search window larger than 64 along some axis is not supported by the 2D kernel";
@@ -640,6 +695,8 @@ cudaError_t launch_piv2d(const Piv2dArgs& a, int alg, cudaStream_t s, std::strin
   const int N = piv2d_fft_len(SS1, SS2);
   const bool prune = (a.IS1 <= N / 2) && (a.IS2 <= N / 2);
   if (piv2d_team_ok(N, prune, alg)) return launch_piv2d_team(a, N, alg, s, err);
+  if (piv2d_local_sums(a.IS1, a.IS2, a.SM1, a.SM2, alg))
+    return N == 64 ? launch_lw<64, 2>(a, alg, s, err) : launch_lw<32, 3>(a, alg, s, err);
   if (N == 64) return prune ? launch_dt<64, true, 4, 2>(a, alg, s, err) : launch_dt<64, false, 4, 2>(a, alg, s, err);
   // length 32 needs fewer registers: three blocks per SM (12 warps) without spill
   if (N == 32) return prune ? launch_dt<32, true, 4, 3>(a, alg, s, err) : launch_dt<32, false, 4, 3>(a, alg, s, err);

@@ -157,6 +157,12 @@ struct Layout2d {
   static MQP_HD MQP_FI int warp_f2(int P1, int P2, bool masked = false) {
     return G_SIZE + region2_f2(P1, P2) + extra_f2(masked, P1, P2);
   }
+  // kernels that form the window sums on chip (lw_rows / lw_cols): the
+  // (N/2 + 1) x N FP64 table overlays the dead G spectra and may run past
+  // them, so their plane starts after the larger of the two
+  static constexpr int TBL = (N / 2 + 1) * N;
+  static constexpr int F_OFF_LW = G_SIZE > TBL ? G_SIZE : TBL;
+  static MQP_HD MQP_FI int warp_f2_lw(int P1, int P2) { return F_OFF_LW + region2_f2(P1, P2); }
 };
 
 // ---------------------------------------------------------------------------
@@ -723,14 +729,134 @@ MQP_HD MQP_FI double similarity_value(const IAScalars& sc, float sqF, double c, 
   return (double)((float)c / (sqrtf((float)SG) * sqF));
 }
 
+// ---------------------------------------------------------------------------
+// window sums on chip (interrogation window = half the FFT length)
+// ---------------------------------------------------------------------------
+// The reference forms sum_win(pad_G^2) for every fully-overlapping lag from
+// an integral array of the IA's squared padded search window
+// (integralArraySQ! and add_numerator_nsqecc, src/utils/common_ops.jl:142-245;
+// pad_G minus the search-region mean for ZNCC, src/utils/zncc_ops.jl:18-25).
+// When the lag window (the interrogation window) is H x H with H = N/2, the
+// warp kernel forms the same sums in FP64 from the window's pixels, in two
+// passes over a table in its own shared memory (the G spectra are dead by
+// then), instead of four lookups per lag in whole-image integral images.  A
+// window [s, s + H) of a length-N line splits at H into the suffix
+// [s, H) of the first half and the prefix [H, H + s) of the second, so each
+// pass is two independent running sums of non-negative terms (no
+// cancellation, half the dependency chain of one sliding sum):
+//   lw_rows  lane = pad row p1 (p1 = lane + 32 h): R[p1][s2] over columns;
+//   lw_cols  lane = lag column s2: S[s1][s2] over rows of R, written over R;
+//            a 33rd column (P2 = H + 1 = 33) by warp scans, lanes over rows.
+// Element (p1, s2) sits at s2 * N + (p1 ^ (s2 & 31)): lanes over p1, over s2
+// and over s1 (the finish) all hit distinct bank pairs.
+MQP_HD MQP_FI int lw_at(int N, int p1, int s2) { return s2 * N + (p1 ^ (s2 & 31)); }
+
+template <int N, typename T, bool ZNCC>
+MQP_HD MQP_FI void lw_rows(const Piv2dArgs& a, const IAGeom& g, double meanG, int lane, int P2, double* lw) {
+  constexpr int H = N / 2;
+  // one row per batch of loads (two rows of 64 live values spill)
+  constexpr int RB = 1;
+#pragma unroll 1
+  for (int h0 = 0; h0 < N / 32; h0 += RB) {
+    T v[RB][N];
+    bool live[RB];
+#pragma unroll
+    for (int b = 0; b < RB; ++b) {
+      const int p1 = lane + 32 * (h0 + b);
+      live[b] = p1 >= g.lo1 && p1 < g.hi1;
+      const T* src = reinterpret_cast<const T*>(a.img2) + ((long long)(g.g01 + p1) + (long long)a.H * g.g02);
+#pragma unroll
+      for (int x = 0; x < N; ++x)
+        v[b][x] = (live[b] && x >= g.lo2 && x < g.hi2) ? ldg_px<T>(src, (long long)a.H * x) : T(0);
+    }
+    mqp_no_hoist();  // every load of the batch is issued before the first use
+#pragma unroll
+    for (int b = 0; b < RB; ++b) {
+      const int p1 = lane + 32 * (h0 + b);
+      // pad_G^2 (0 outside the clipped search region)
+      auto q = [&](int x) {
+        const double d = ZNCC ? (double)v[b][x] - meanG : (double)v[b][x];
+        return (live[b] && x >= g.lo2 && x < g.hi2) ? d * d : 0.0;
+      };
+      double A[H + 1];  // A[s] = sum of q over [s, H)
+      A[H] = 0.0;
+#pragma unroll
+      for (int x = H - 1; x >= 0; --x) A[x] = A[x + 1] + q(x);
+      double B = 0.0;  // sum of q over [H, H + s2)
+#pragma unroll
+      for (int s2 = 0; s2 <= H; ++s2) {
+        if (s2 < P2) lw[lw_at(N, p1, s2)] = A[s2] + B;
+        if (s2 < H) B = B + q(H + s2);
+      }
+    }
+  }
+}
+
+template <int N>
+MQP_HD MQP_FI void lw_cols(int lane, int P1, int P2, double* lw) {
+  constexpr int H = N / 2;
+  const int s2 = lane;
+  if (s2 < P2) {
+    const int sw = s2 & 31;
+    double* col = lw + s2 * N;
+    double r[N];
+#pragma unroll
+    for (int p = 0; p < N; ++p) r[p] = col[p ^ sw];
+    double A[H + 1];  // A[s1] = sum of r over [s1, H)
+    A[H] = 0.0;
+#pragma unroll
+    for (int p = H - 1; p >= 0; --p) A[p] = A[p + 1] + r[p];
+    double B = 0.0;
+#pragma unroll
+    for (int s1 = 0; s1 <= H; ++s1) {
+      if (s1 < P1) col[s1 ^ sw] = A[s1] + B;
+      if (s1 < H) B = B + r[H + s1];
+    }
+  }
+}
+
+// Column 32 of lw_cols (N = 64, P2 = 33): lanes over rows, r0 = R[lane],
+// r1 = R[32 + lane]; S[s1] = (rows [s1, 32)) + (rows [32, 32 + s1)) by two
+// log-step scans.  The scan steps, shared with the host emulation:
+MQP_HD MQP_FI void lw_scan_step(double& suf, double& pre, double suf_from_above, double pre_from_below, int lane,
+                                int off) {
+  if (lane + off < 32) suf += suf_from_above;
+  if (lane >= off) pre += pre_from_below;
+}
+template <int N>
+MQP_HD MQP_FI void lw_col32(int lane, int P1, int P2, double* lw) {
+#if defined(__CUDA_ARCH__)
+  if (N != 64 || P2 <= 32) return;
+  double* col = lw + 32 * N;  // (p1 ^ (32 & 31)) = p1: no swizzle in this column
+  const double r0 = col[lane], r1 = col[lane + 32];
+  __syncwarp();
+  double suf = r0, pre = r1;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const double a = __shfl_down_sync(0xffffffffu, suf, off);
+    const double b = __shfl_up_sync(0xffffffffu, pre, off);
+    lw_scan_step(suf, pre, a, b, lane, off);
+  }
+  double ex = __shfl_up_sync(0xffffffffu, pre, 1);  // rows [32, 32 + lane)
+  if (lane == 0) ex = 0.0;
+  if (lane < P1) col[lane] = suf + ex;
+  if (lane == 31 && P1 > 32) col[32] = pre;  // S[32]: rows [32, 64)
+#else
+  (void)lane, (void)P1, (void)P2, (void)lw;  // the host emulation runs the scan lane by lane
+#endif
+}
+
 // Finishes lag row s1: prow[s2] (s2 < P2) holds the raw correlation on entry
 // and the similarity on exit; the row's elements enter the peak / SN
 // accumulators.  Window sums come from the FP64 integral images of img2 and
 // img2^2; lanes are consecutive lag rows, so each lookup is a coalesced
 // column segment, and four lags' lookups are issued before any is used.
-template <int ALG>
+// LWN = N: the window sums come from the on-chip table lw (lw_rows /
+// lw_cols; for ZNCC already about the search mean), not from the images.
+template <int ALG, int LWN = 0>
 MQP_HD MQP_FI void finish_row(const Piv2dArgs& a, const IAGeom& g, const IAScalars& sc, int s1, int P1,
-                              int P2, double* prow, const LagRanges& R, PeakAcc& acc, const float* c1row = nullptr) {
+                              int P2, double* prow, const LagRanges& R, PeakAcc& acc, const float* c1row = nullptr,
+                              const double* lw = nullptr) {
   const float sqF = sqrtf((float)sc.sumF2);
   if (ALG == ALG_MASK_NSQECC) {
     // prow holds mask*G^2, c1row the parked (F*mask)*G
@@ -752,7 +878,9 @@ MQP_HD MQP_FI void finish_row(const Piv2dArgs& a, const IAGeom& g, const IAScala
       S1v[t] = 0.0;
       nv[t] = 0.0;
       const int s2 = b + t;
-      if (ALG != ALG_FFTCC && s2 < P2) {
+      if (LWN && s2 < P2) {
+        S2v[t] = lw[lw_at(LWN, s1, s2)];
+      } else if (ALG != ALG_FFTCC && s2 < P2) {
         int c0, c1;
         lag_window(s2, a.IS2, g.g02, g.lo2, g.hi2, c0, c1);
         if (r1 > r0 && c1 > c0) {
@@ -782,10 +910,11 @@ MQP_HD MQP_FI void finish_row(const Piv2dArgs& a, const IAGeom& g, const IAScala
 
 // One element (s1, s2) of a tail lag row (the whole warp shares such rows,
 // lanes over s2); c is the raw correlation.
-template <int ALG>
+template <int ALG, int LWN = 0>
 MQP_HD MQP_FI double finish_one(const Piv2dArgs& a, const IAGeom& g, const IAScalars& sc, int s1, int s2,
-                                double c, double cmask = 0.0) {
+                                double c, double cmask = 0.0, const double* lw = nullptr) {
   if (ALG == ALG_FFTCC) return c;
+  if (LWN) return similarity_value<ALG>(sc, sqrtf((float)sc.sumF2), c, lw[lw_at(LWN, s1, s2)], 0.0, 0.0);
   // masked: c = mask*G^2, cmask = (F*mask)*G
   if (ALG == ALG_MASK_NSQECC) return similarity_value<ALG>(sc, sqrtf((float)sc.sumF2), cmask, c, 0.0, 0.0);
   int r0, r1, c0, c1;

@@ -36,16 +36,10 @@
 
 namespace mqp {
 
-// An empty asm statement with a memory clobber: loads after it cannot move
-// above it.  Each half-specialised phase function starts with one, so the
-// compiler keeps the two halves' identical loads inside their branches of
-// the warp-uniform dispatch instead of hoisting them (which holds both
+// mqp_no_hoist (mqp_fft.cuh) opens each half-specialised phase function, so
+// the compiler keeps the two halves' identical loads inside their branches
+// of the warp-uniform dispatch instead of hoisting them (which holds both
 // halves' data live and spills).
-MQP_HD MQP_FI void mqp_no_hoist() {
-#if defined(__CUDA_ARCH__)
-  asm volatile("" ::: "memory");
-#endif
-}
 
 // Shared-memory layout of one team (float2 units).
 //   G region: spectrum columns u = 0..M-1 of the G rows (stride GS = N + 1 over

@@ -31,14 +31,15 @@ static void integral(const void* img, int dtype, int H, int W, bool sq, std::vec
   }
 }
 
-template <int N, bool FPRUNE, int ALG, typename T>
+template <int N, bool FPRUNE, int ALG, typename T, bool LW = false>
 static void emu_ia(const Piv2dArgs& a, long long ia, std::vector<float2>& ws) {
   using Lay = Layout2d<N, FPRUNE>;
   constexpr int M = N / 2;
   constexpr bool MASKED = ALG == ALG_MASK_NSQECC;
   const int P1 = 2 * a.SM1 + 1, P2 = 2 * a.SM2 + 1;
   float2* GH = ws.data();
-  float2* FH = GH + Lay::F_OFF;
+  float2* FH = GH + (LW ? Lay::F_OFF_LW : Lay::F_OFF);
+  double* lw = LW ? reinterpret_cast<double*>(GH) : nullptr;
   double* plane = reinterpret_cast<double*>(FH);
   float* c1buf = MASKED ? reinterpret_cast<float*>(FH + Lay::region2_f2(P1, P2)) : nullptr;
   float2 tw[N];
@@ -106,6 +107,31 @@ static void emu_ia(const Piv2dArgs& a, long long ia, std::vector<float2>& ws) {
     }
     for (int s1 = lane_rows; s1 < P1; ++s1)
       for (int s2 = 0; s2 < P2; ++s2) plane[s1 * P2 + s2] = (double)tail_row_value<N, FPRUNE>(GH, tw, s1, s2) * scale;
+    if (LW) {
+      // the on-chip window sums: every lane's rows, then every lane's columns
+      for (int lane = 0; lane < 32; ++lane) lw_rows<N, T, ALG == ALG_ZNCC>(a, g, sc.meanG, lane, P2, lw);
+      for (int lane = 0; lane < 32; ++lane) lw_cols<N>(lane, P1, P2, lw);
+      if (N == 64 && P2 > 32) {
+        // lw_col32's warp scans, lane by lane
+        double* col = lw + 32 * N;
+        double suf[32], pre[32], r1[32];
+        for (int l = 0; l < 32; ++l) {
+          suf[l] = col[l];
+          pre[l] = r1[l] = col[l + 32];
+        }
+        for (int off = 1; off < 32; off <<= 1) {
+          double a_[32], b_[32];
+          for (int l = 0; l < 32; ++l) {
+            a_[l] = l + off < 32 ? suf[l + off] : suf[l];
+            b_[l] = l >= off ? pre[l - off] : pre[l];
+          }
+          for (int l = 0; l < 32; ++l) lw_scan_step(suf[l], pre[l], a_[l], b_[l], l, off);
+        }
+        for (int l = 0; l < 32 && l < P1; ++l) col[l] = suf[l] + (l ? pre[l - 1] : 0.0);
+        if (P1 > 32) col[32] = pre[31];
+        (void)r1;
+      }
+    }
     if (MASKED && pass == 0)
       for (int i = 0; i < P1 * P2; ++i) c1buf[i] = (float)plane[i];
   }
@@ -125,11 +151,12 @@ static void emu_ia(const Piv2dArgs& a, long long ia, std::vector<float2>& ws) {
     acc.smax = -INFINITY;
     acc.ssum = 0.0;
     for (int s1 = lane; s1 < lane_rows; s1 += 32)
-      finish_row<ALG>(a, g, sc, s1, P1, P2, plane + s1 * P2, R, acc, MASKED ? c1buf + s1 * P2 : nullptr);
+      finish_row<ALG, LW ? N : 0>(a, g, sc, s1, P1, P2, plane + s1 * P2, R, acc, MASKED ? c1buf + s1 * P2 : nullptr,
+                                  lw);
     for (int s1 = lane_rows; s1 < P1; ++s1)
       for (int s2 = lane; s2 < P2; s2 += 32) {
         double& e = plane[s1 * P2 + s2];
-        e = finish_one<ALG>(a, g, sc, s1, s2, e, MASKED ? (double)c1buf[s1 * P2 + s2] : 0.0);
+        e = finish_one<ALG, LW ? N : 0>(a, g, sc, s1, s2, e, MASKED ? (double)c1buf[s1 * P2 + s2] : 0.0, lw);
         acc_take(acc, R, s1, s2, P1, e);
       }
     peak_merge(best, bidx, acc.best, acc.bidx);
@@ -152,14 +179,24 @@ static void emu_ia(const Piv2dArgs& a, long long ia, std::vector<float2>& ws) {
   if (a.SN) a.SN[vfo] = sn;
 }
 
-template <int N, bool FPRUNE, int ALG>
+template <int N, bool FPRUNE, int ALG, bool LW = false>
 static void emu_run(const Piv2dArgs& a) {
   using Lay = Layout2d<N, FPRUNE>;
-  std::vector<float2> ws((size_t)Lay::warp_f2(2 * a.SM1 + 1, 2 * a.SM2 + 1, ALG == ALG_MASK_NSQECC));
+  const int P1 = 2 * a.SM1 + 1, P2 = 2 * a.SM2 + 1;
+  std::vector<float2> ws((size_t)(LW ? Lay::warp_f2_lw(P1, P2) : Lay::warp_f2(P1, P2, ALG == ALG_MASK_NSQECC)));
   for (long long ia = a.ia_begin; ia < a.ia_end; ++ia) {
-    if (a.dtype == 0) emu_ia<N, FPRUNE, ALG, float>(a, ia, ws);
-    else emu_ia<N, FPRUNE, ALG, double>(a, ia, ws);
+    if (a.dtype == 0) emu_ia<N, FPRUNE, ALG, float, LW>(a, ia, ws);
+    else emu_ia<N, FPRUNE, ALG, double, LW>(a, ia, ws);
   }
+}
+
+// ZNCC with the on-chip window sums (launch_piv2d's choice for an N/2 x N/2
+// interrogation window)
+template <int N>
+static int emu_lw(const Piv2dArgs& a, int alg) {
+  if (alg != 1) return -1;
+  emu_run<N, true, 1, true>(a);
+  return 0;
 }
 
 // The team kernel (mqp_piv2d_team.cuh) thread by thread: each phase runs for
@@ -295,6 +332,19 @@ extern "C" __attribute__((visibility("default"))) int mqp_emu_piv2d(
     int IS1, int IS2, int SM1, int SM2, int st1, int st2, int alg, double threshold, double mask_threshold,
     int computeSN, double* VF, double* SN, double* planes, long long ia_begin, long long ia_end) {
   std::vector<double> II1, IIg, IIg2;
+  const int SS = (IS1 + 2 * SM1) > (IS2 + 2 * SM2) ? (IS1 + 2 * SM1) : (IS2 + 2 * SM2);
+  const int N = SS <= 32 ? 32 : (SS <= 64 ? 64 : (SS <= 128 ? 128 : (SS <= 256 ? 256 : 0)));
+  const bool prune = IS1 <= N / 2 && IS2 <= N / 2;
+  // MQP_EMU_PIV2D_TEAM=1 emulates the opt-in team kernel for pruned FFTCC /
+  // ZNCC / NSQECC (default: the one-warp-per-IA kernel, as launch_piv2d);
+  // MQP_EMU_PIV2D_NO_LW=1 keeps the integral-image window sums where the warp
+  // kernel forms them on chip
+  const char* team_env = getenv("MQP_EMU_PIV2D_TEAM");
+  const char* nolw_env = getenv("MQP_EMU_PIV2D_NO_LW");
+  const bool direct = direct2d_ok(IS1, IS2, SM1, SM2);
+  const bool team = !direct && prune && alg <= 2 && (N == 32 || N == 64) && team_env && team_env[0] == '1';
+  const bool lw = !direct && !team && alg == 1 && (N == 32 || N == 64) && IS1 == N / 2 &&
+                  IS2 == N / 2 && !(nolw_env && nolw_env[0] == '1');
   Piv2dArgs a;
   memset(&a, 0, sizeof(a));
   a.img1 = img1;
@@ -303,7 +353,7 @@ extern "C" __attribute__((visibility("default"))) int mqp_emu_piv2d(
   a.mask_skip = mask_skip;
   a.mask_threshold = mask_threshold;
   a.dtype = dtype;
-  if (alg == 1 || alg == 2) {
+  if ((alg == 1 || alg == 2) && !lw) {  // the on-chip sums read no img2^2 integral
     integral(img2, dtype, H, W, true, IIg2);
     a.IIg2 = IIg2.data();
   }
@@ -323,16 +373,10 @@ extern "C" __attribute__((visibility("default"))) int mqp_emu_piv2d(
   a.ia_end = ia_end;
   a.threshold = threshold;
   a.computeSN = computeSN;
-  const int SS = (IS1 + 2 * SM1) > (IS2 + 2 * SM2) ? (IS1 + 2 * SM1) : (IS2 + 2 * SM2);
-  const int N = SS <= 32 ? 32 : (SS <= 64 ? 64 : (SS <= 128 ? 128 : (SS <= 256 ? 256 : 0)));
-  const bool prune = IS1 <= N / 2 && IS2 <= N / 2;
-  if (direct2d_ok(IS1, IS2, SM1, SM2)) return emu_piv2d_direct(a, alg);
+  if (direct) return emu_piv2d_direct(a, alg);
   if (N == 128) return emu_piv2d_big(a, alg);
   if (N == 256) return IS1 <= 128 && IS2 <= 128 ? emu_piv2d_huge(a, alg) : -2;
-  // the team kernel (launch_piv2d's opt-in variant) for pruned FFTCC / ZNCC /
-  // NSQECC; MQP_EMU_PIV2D_WARP=1 emulates the one-warp-per-IA kernel for them
-  const char* warp_env = getenv("MQP_EMU_PIV2D_WARP");
-  const bool team = prune && alg <= 2 && !(warp_env && warp_env[0] == '1');
+  if (lw) return N == 64 ? emu_lw<64>(a, alg) : emu_lw<32>(a, alg);
   if (N == 64) return team ? emu_team<64>(a, alg) : (prune ? emu_alg<64, true>(a, alg) : emu_alg<64, false>(a, alg));
   if (N == 32) return team ? emu_team<32>(a, alg) : (prune ? emu_alg<32, true>(a, alg) : emu_alg<32, false>(a, alg));
   return -2;

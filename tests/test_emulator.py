@@ -203,7 +203,7 @@ def test_emulated_team_and_warp_kernels_agree(emu, alg, cfg, monkeypatch):
     VFo, SNo, Co = O.piv_single_pass(i1, i2, po, keep_corr=True)
     out = {}
     for mode in ("team", "warp"):
-        monkeypatch.setenv("MQP_EMU_PIV2D_WARP", "1" if mode == "warp" else "0")
+        monkeypatch.setenv("MQP_EMU_PIV2D_TEAM", "1" if mode == "team" else "0")
         VF, SN, PL = run_emu(emu, i1, i2, alg, IS, SM, st)
         worst, near_tie = compare_planes(PL, Co, i1.shape, IS, SM, st)
         assert worst <= PLANE_RTOL, (mode, worst)
@@ -234,3 +234,35 @@ def test_emulated_window256_kernel_matches_oracle(emu, alg, cfg):
     bad = (np.abs(VF - VFo) > VF_ATOL).any(axis=0) & ~near_tie
     assert not bad.any()
     assert (sn_ok(SN, SNo, sn_condition(Co, i1.shape, IS, SM, st)) | near_tie).all()
+
+
+@pytest.mark.parametrize("alg", ["zncc"])
+@pytest.mark.parametrize("cfg", [((32, 32), (16, 16), (8, 8)), ((16, 16), (8, 8), (8, 8)), ((32, 32), (9, 13), (12, 16)),
+                                 ((16, 16), (5, 3), (6, 10))])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_emulated_onchip_window_sums(emu, alg, cfg, dtype, monkeypatch):
+    """ZNCC with an interrogation window of half the FFT length takes its
+    window sums from an on-chip table built from the pixels (lw_rows /
+    lw_cols) instead of integral images: both routes match the oracle and
+    each other to FP64 rounding in the sums."""
+    IS, SM, st = cfg
+    i1, i2, _ = synth.pair_2d_vortex(shape=(130, 118), seed_stream=29, core=35.0)
+    i1, i2 = i1.astype(dtype), i2.astype(dtype)
+    po = O.set_piv_parameters(corr_alg=alg, interSize=IS, searchMargin=SM, step=st, computeSN=True)
+    po.ndims = 2
+    VFo, SNo, Co = O.piv_single_pass(i1, i2, po, keep_corr=True)
+    out = {}
+    for mode in ("lw", "integral"):
+        monkeypatch.setenv("MQP_EMU_PIV2D_NO_LW", "1" if mode == "integral" else "0")
+        VF, SN, PL = run_emu(emu, i1, i2, alg, IS, SM, st)
+        worst, near_tie = compare_planes(PL, Co, i1.shape, IS, SM, st)
+        assert worst <= PLANE_RTOL, (mode, worst)
+        bad = (np.abs(VF - VFo) > VF_ATOL).any(axis=0) & ~near_tie
+        assert not bad.any(), mode
+        assert (sn_ok(SN, SNo, sn_condition(Co, i1.shape, IS, SM, st)) | near_tie).all(), mode
+        out[mode] = (VF, PL)
+    fin = np.isfinite(out["lw"][1])
+    assert np.array_equal(fin, np.isfinite(out["integral"][1]))
+    scale = np.max(np.abs(out["lw"][1][fin]))
+    assert np.max(np.abs(out["lw"][1][fin] - out["integral"][1][fin])) <= 3e-7 * scale  # FP32 quotient: an ulp or two
+    assert np.max(np.abs(out["lw"][0] - out["integral"][0])) < 1e-5
