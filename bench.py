@@ -326,7 +326,7 @@ def run_ours(args):
         traffic = tr["dram_bytes_per_launch"] * n_ia / tr["ia_per_launch"]
     except Exception:
         pass
-    kname = ("piv2d_kernel (one IA per warp, FFT length 64)" if nd == 2
+    kname = ("piv2d_kernel (one IA per warp, FFT length 64, search windows staged by TMA)" if nd == 2
              else "k3a_kernel + k3b_kernel + k3c_kernel (all chunks of one pass)")
     roof = {"bound": "fp32", "kernel": kname, "achieved": achieved / 1e12, "peak": fp32_peak / 1e12,
             "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": traffic,

@@ -3,10 +3,13 @@
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
 
 #include <string>
 
 #include "mqp_internal.h"
+#include "mqp_stage.cuh"
 
 namespace mqp {
 
@@ -254,15 +257,31 @@ __device__ __forceinline__ void warp_peak(double& best, int& bidx) {
 // warp.  GH is the warp's shared-memory workspace (Layout2d, sized for this
 // IA's lag plane), tw the (cos, sin)(2 pi j / N) table.  LW: ZNCC with an
 // N/2 x N/2 interrogation window forms its window sums on chip (lw_rows /
-// lw_cols) instead of reading integral images.
-template <int N, bool FPRUNE, int ALG, typename T, bool LW = false>
-__device__ __forceinline__ void piv2d_ia(const Piv2dArgs& a, long long ia, float2* GH, const float2* tw, int lane) {
+// lw_cols) instead of reading integral images.  STG: this IA's search window
+// was staged into GH by the TMA (mqp_stage.cuh) on mbar's phase `phase`, and
+// the IA stages window ia_next (>= 0) as soon as its own G spectra are dead.
+template <int N, bool FPRUNE, int ALG, typename T, bool LW = false, bool STG = false>
+__device__ __forceinline__ void piv2d_ia(const Piv2dArgs& a, long long ia, float2* GH, const float2* tw, int lane,
+                                         const CUtensorMap* tmap = nullptr, uint64_t* mbar = nullptr,
+                                         unsigned* phase = nullptr, long long ia_next = -1) {
   using Lay = Layout2d<N, FPRUNE>;
   constexpr int M = N / 2;
   constexpr bool MASKED = ALG == ALG_MASK_NSQECC;
   static_assert(!LW || ((ALG == ALG_ZNCC || ALG == ALG_NSQECC) && FPRUNE), "on-chip window sums: ZNCC / NSQECC");
+  static_assert(!STG || (!LW && !MASKED && sizeof(T) == 4), "staged windows: FP32, unmasked, integral-image sums");
   const int P1 = 2 * a.SM1 + 1, P2 = 2 * a.SM2 + 1;
-  float2* FH = GH + (LW ? Lay::F_OFF_LW : Lay::F_OFF);
+  float2* FH = GH + (LW ? Lay::F_OFF_LW : (STG ? Lay::F_OFF_STG : Lay::F_OFF));
+  // the next IA's window into the dead G spectra (every lane calls it)
+  auto stage_next = [&]() {
+    if (STG && ia_next >= 0 && *phase != STAGE_OFF) {
+      stage_fence();
+      __syncwarp();
+      if (lane == 0) {
+        const IAGeom gn = ia_geom(a, (int)(ia_next % a.vf1), (int)(ia_next / a.vf1));
+        stage_issue<N>(tmap, reinterpret_cast<float*>(GH), mbar, stage_x0(gn.g01), gn.g02);
+      }
+    }
+  };
   double* lw = LW ? reinterpret_cast<double*>(GH) : nullptr;
   double* plane = reinterpret_cast<double*>(FH);
   float* c1buf = MASKED ? reinterpret_cast<float*>(FH + Lay::region2_f2(P1, P2)) : nullptr;
@@ -299,6 +318,50 @@ __device__ __forceinline__ void piv2d_ia(const Piv2dArgs& a, long long ia, float
     // transformed.
     constexpr int NJF = (Lay::NF + 31) / 32, NJ = NJF + N / 32;
     double vmax = -INFINITY, mmax = -INFINITY, sumsq = 0.0;
+    if (STG) {
+      // F rows from global memory (row_process reads them itself) while the
+      // staged window lands; then every lane reads its G rows from the tile
+      // before any lane writes spectra over it
+#pragma unroll 1
+      for (int job = 0; job < NJF; ++job) {
+        const RowJob jf = row_job<N, FPRUNE>(a, g, lane, job);
+        float none[N];
+#pragma unroll
+        for (int x = 0; x < N; ++x) none[x] = 0.f;
+        if (jf.row < Lay::NF) row_process<N, FPRUNE, T, ALG == ALG_ZNCC>(a, sc, pmode, jf, none, GH, FH, vmax, mmax, sumsq);
+      }
+      // a copy that never lands (bounded wait) raises the status flag and
+      // turns staging off for this warp: its rows come from global memory
+      const bool armed = *phase != STAGE_OFF;
+      const bool tiled = __all_sync(0xffffffffu, armed && stage_wait(mbar, *phase));  // one verdict per warp
+      if (armed) {
+        if (tiled) {
+          *phase ^= 1u;
+        } else {
+          *phase = STAGE_OFF;
+          if (a.status && lane == 0) atomicExch(a.status, 1);
+        }
+      }
+      const float* tile = reinterpret_cast<const float*>(GH) + (g.g01 - stage_x0(g.g01));
+      float gv[N / 32][N];
+      RowJob jg[N / 32];
+#pragma unroll
+      for (int h = 0; h < N / 32; ++h) {
+        jg[h] = row_job<N, FPRUNE>(a, g, lane, NJF + h);
+        if (tiled) {
+          const float* rowp = tile + jg[h].row;
+#pragma unroll
+          for (int x = 0; x < N; ++x)
+            gv[h][x] = (jg[h].live && x >= jg[h].xlo && x < jg[h].xhi) ? rowp[x * StageTile<N>::ROWS] : 0.f;
+        } else {
+          row_load<N, T>(a, jg[h], gv[h]);
+        }
+      }
+      __syncwarp();
+#pragma unroll 1
+      for (int h = 0; h < N / 32; ++h)
+        row_process<N, FPRUNE, T, ALG == ALG_ZNCC>(a, sc, pmode, jg[h], gv[h], GH, FH, vmax, mmax, sumsq);
+    } else {
     float buf[N];
     RowJob jn = row_job<N, FPRUNE>(a, g, lane, 0);
     row_load<N, T>(a, jn, buf);
@@ -314,6 +377,7 @@ __device__ __forceinline__ void piv2d_ia(const Piv2dArgs& a, long long ia, float
       }
       if (!(jc.isF && jc.row >= Lay::NF))
         row_process<N, FPRUNE, T, ALG == ALG_ZNCC>(a, sc, pmode, jc, cur, GH, FH, vmax, mmax, sumsq);
+    }
     }
     if (pass == 0) {
       vmax = warp_max(vmax);
@@ -382,6 +446,7 @@ __device__ __forceinline__ void piv2d_ia(const Piv2dArgs& a, long long ia, float
       for (int s2 = lane; s2 < P2; s2 += 32)
         plane[s1 * P2 + s2] = (double)tail_row_value<N, FPRUNE>(GH, tw, s1, s2) * scale;
     __syncwarp();
+    stage_next();
     if (LW) {
       // the G spectra are dead: their space takes the window-sum table
       lw_rows<N, T, ALG == ALG_ZNCC>(a, g, sc.meanG, lane, P2, lw);
@@ -397,6 +462,7 @@ __device__ __forceinline__ void piv2d_ia(const Piv2dArgs& a, long long ia, float
     }
   }
   if (skipped) {
+    stage_next();
     if (lane == 0) {
       a.VF[2 * vfo + 0] = 0.0;
       a.VF[2 * vfo + 1] = 0.0;
@@ -463,21 +529,32 @@ __device__ __forceinline__ void piv2d_ia(const Piv2dArgs& a, long long ia, float
 // Persistent: each warp walks IAs ia = first + k * (all warps).  The warp's
 // shared-memory workspace holds the spectra rows of G (N/2 x (N+1)) and F
 // (N/2 x (NF+1)); after phase 2 the F rows are reused for the FP64 plane.
-template <int N, bool FPRUNE, int ALG, typename T, int WARPS, int MINB, bool LW = false>
-__global__ void __launch_bounds__(WARPS * 32, MINB) piv2d_kernel(Piv2dArgs a) {
-  extern __shared__ float2 smem[];
+// STG: tmap describes img2 for the staged windows (mqp_stage.cuh); each
+// warp stages its first window before the loop and every IA the next one.
+template <int N, bool FPRUNE, int ALG, typename T, int WARPS, int MINB, bool LW = false, bool STG = false>
+__global__ void __launch_bounds__(WARPS * 32, MINB) piv2d_kernel(Piv2dArgs a, const __grid_constant__ CUtensorMap tmap) {
+  extern __shared__ __align__(128) float2 smem[];
   using Lay = Layout2d<N, FPRUNE>;
   constexpr bool MASKED = ALG == ALG_MASK_NSQECC;
   const int P1 = 2 * a.SM1 + 1, P2 = 2 * a.SM2 + 1;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int wf2 = LW ? Lay::warp_f2_lw(P1, P2) : Lay::warp_f2(P1, P2, MASKED);
+  const int wf2 = LW ? Lay::warp_f2_lw(P1, P2) : (STG ? Lay::warp_f2_stg(P1, P2) : Lay::warp_f2(P1, P2, MASKED));
   float2* GH = smem + (size_t)warp * wf2;
   float2* tw = smem + (size_t)WARPS * wf2;  // (cos, sin)(2 pi j / N)
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(tw + N) + warp;
   for (int j = threadIdx.x; j < N; j += blockDim.x) tw[j] = twiddle_rt(j * (TW_N / N));
+  if (STG && lane == 0) stage_init(mbar);
   __syncthreads();
   const long long nwarps = (long long)gridDim.x * WARPS;
-  for (long long ia = a.ia_begin + (long long)blockIdx.x * WARPS + warp; ia < a.ia_end; ia += nwarps)
-    piv2d_ia<N, FPRUNE, ALG, T, LW>(a, ia, GH, tw, lane);
+  const long long first = a.ia_begin + (long long)blockIdx.x * WARPS + warp;
+  unsigned phase = 0;
+  if (STG && first < a.ia_end && lane == 0) {
+    const IAGeom g0 = ia_geom(a, (int)(first % a.vf1), (int)(first / a.vf1));
+    stage_issue<N>(&tmap, reinterpret_cast<float*>(GH), mbar, stage_x0(g0.g01), g0.g02);
+  }
+  for (long long ia = first; ia < a.ia_end; ia += nwarps)
+    piv2d_ia<N, FPRUNE, ALG, T, LW, STG>(a, ia, GH, tw, lane, &tmap, mbar, &phase,
+                                         ia + nwarps < a.ia_end ? ia + nwarps : -1);
 }
 
 // Batched: the IAs of many image pairs sharing one kernel variant form one
@@ -532,13 +609,57 @@ int device_sm_count(int device) {
   return n;
 }
 
-template <int N, bool FPRUNE, int ALG, typename T, int WARPS, int MINB, bool LW = false>
-static cudaError_t launch_t(const Piv2dArgs& a, cudaStream_t s, std::string& err) {
+// Tensor map of an H x W column-major FP32 image for the staged windows of
+// FFT length N: dim 0 = rows (contiguous), dim 1 = columns, box (N + 4) x N,
+// zero fill outside the image.  False when the image does not qualify (row
+// pitch not a multiple of 16 bytes, base not 16-byte aligned) or the driver
+// entry point is missing; the caller then launches the unstaged kernel.
+static bool stage_tensor_map(CUtensorMap* m, const void* img, long long H, long long W, int N) {
+  if (H % 4 != 0 || ((uintptr_t)img & 15) != 0 || H < 1 || W < 1) return false;
+  typedef CUresult (*EncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static EncodeTiled encode = nullptr;
+  static bool looked = false;
+  if (!looked) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      encode = (EncodeTiled)fn;
+    looked = true;
+  }
+  if (!encode) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)H, (cuuint64_t)W};
+  const cuuint64_t strides[1] = {(cuuint64_t)H * 4};
+  const cuuint32_t box[2] = {(cuuint32_t)(N + 4), (cuuint32_t)N};
+  const cuuint32_t estr[2] = {1, 1};
+  return encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void*>(img), dims, strides, box, estr,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Staged windows are on unless MQP_TUNE_PIV2D_TMA=0 (both kernels give
+// identical results; the knob exists for timing comparisons).
+static bool stage_enabled() {
+  static int on = -1;
+  if (on < 0) {
+    const char* v = getenv("MQP_TUNE_PIV2D_TMA");
+    on = (v && v[0] == '0') ? 0 : 1;
+  }
+  return on == 1;
+}
+
+template <int N, bool FPRUNE, int ALG, typename T, int WARPS, int MINB, bool LW = false, bool STG = false>
+static cudaError_t launch_t(const Piv2dArgs& a, cudaStream_t s, std::string& err, const CUtensorMap* tm = nullptr) {
   using Lay = Layout2d<N, FPRUNE>;
   const int P1 = 2 * a.SM1 + 1, P2 = 2 * a.SM2 + 1;
-  const int wf2 = LW ? Lay::warp_f2_lw(P1, P2) : Lay::warp_f2(P1, P2, ALG == ALG_MASK_NSQECC);
-  const size_t smem = ((size_t)WARPS * wf2 + N) * sizeof(float2);
-  auto kern = piv2d_kernel<N, FPRUNE, ALG, T, WARPS, MINB, LW>;
+  const int wf2 = LW ? Lay::warp_f2_lw(P1, P2) : (STG ? Lay::warp_f2_stg(P1, P2) : Lay::warp_f2(P1, P2, ALG == ALG_MASK_NSQECC));
+  const size_t smem = ((size_t)WARPS * wf2 + N + (STG ? WARPS : 0)) * sizeof(float2);
+  auto kern = piv2d_kernel<N, FPRUNE, ALG, T, WARPS, MINB, LW, STG>;
+  CUtensorMap tmap;
+  memset(&tmap, 0, sizeof(tmap));
+  if (tm) tmap = *tm;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) {
     err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e);
@@ -557,10 +678,26 @@ static cudaError_t launch_t(const Piv2dArgs& a, cudaStream_t s, std::string& err
   const long long need = (n_ia + WARPS - 1) / WARPS;
   if (blocks > need) blocks = need;
   if (blocks < 1) return cudaSuccess;
-  kern<<<(unsigned)blocks, WARPS * 32, smem, s>>>(a);
+  kern<<<(unsigned)blocks, WARPS * 32, smem, s>>>(a, tmap);
   e = cudaGetLastError();
   if (e != cudaSuccess) err = std::string("piv2d launch: ") + cudaGetErrorString(e);
   return e;
+}
+
+// FP32 FFTCC / NSQECC with staged windows when img2 qualifies.  Measured on
+// B200 (2048^2 vortex, step 8, whole pass): NSQECC interSize 32 2.41 ->
+// 2.31 ms, 24 2.05 -> 1.97, 16 0.86 -> 0.82; FFTCC 32 1.43 -> 1.39, 16 0.65
+// -> 0.52.  ZNCC at interSize 24 ran 2.52 -> 3.23 ms staged (its eight
+// integral-image lookups per lag meet the in-flight copy), so ZNCC loads its
+// rows itself.
+template <int N, bool FPRUNE, int WARPS, int MINB>
+static bool launch_stg(const Piv2dArgs& a, int alg, cudaStream_t s, std::string& err, cudaError_t& e) {
+  if (a.dtype != 0 || !stage_enabled() || (alg != ALG_FFTCC && alg != ALG_NSQECC)) return false;
+  CUtensorMap tm;
+  if (!stage_tensor_map(&tm, a.img2, a.H, a.W, N)) return false;
+  e = alg == ALG_FFTCC ? launch_t<N, FPRUNE, ALG_FFTCC, float, WARPS, MINB, false, true>(a, s, err, &tm)
+                       : launch_t<N, FPRUNE, ALG_NSQECC, float, WARPS, MINB, false, true>(a, s, err, &tm);
+  return true;
 }
 
 template <int N, bool FPRUNE, typename T, int WARPS, int MINB>
@@ -697,6 +834,11 @@ cudaError_t launch_piv2d(const Piv2dArgs& a, int alg, cudaStream_t s, std::strin
   if (piv2d_team_ok(N, prune, alg)) return launch_piv2d_team(a, N, alg, s, err);
   if (piv2d_local_sums(a.IS1, a.IS2, a.SM1, a.SM2, alg))
     return N == 64 ? launch_lw<64, 2>(a, alg, s, err) : launch_lw<32, 3>(a, alg, s, err);
+  cudaError_t e = cudaSuccess;
+  if (N == 64 && (prune ? launch_stg<64, true, 4, 2>(a, alg, s, err, e) : launch_stg<64, false, 4, 2>(a, alg, s, err, e)))
+    return e;
+  if (N == 32 && (prune ? launch_stg<32, true, 4, 3>(a, alg, s, err, e) : launch_stg<32, false, 4, 3>(a, alg, s, err, e)))
+    return e;
   if (N == 64) return prune ? launch_dt<64, true, 4, 2>(a, alg, s, err) : launch_dt<64, false, 4, 2>(a, alg, s, err);
   // length 32 needs fewer registers: three blocks per SM (12 warps) without spill
   if (N == 32) return prune ? launch_dt<32, true, 4, 3>(a, alg, s, err) : launch_dt<32, false, 4, 3>(a, alg, s, err);

@@ -163,6 +163,12 @@ struct Layout2d {
   static constexpr int TBL = (N / 2 + 1) * N;
   static constexpr int F_OFF_LW = G_SIZE > TBL ? G_SIZE : TBL;
   static MQP_HD MQP_FI int warp_f2_lw(int P1, int P2) { return F_OFF_LW + region2_f2(P1, P2); }
+  // kernels that stage the next search window with the TMA (mqp_stage.cuh):
+  // the (N + 4) x N FP32 tile lands over the dead G spectra and may run past
+  // them; each warp's region starts on a 128-byte boundary
+  static constexpr int TILE_F2 = ((N + 4) * N + 1) / 2;
+  static constexpr int F_OFF_STG = G_SIZE > TILE_F2 ? G_SIZE : TILE_F2;
+  static MQP_HD MQP_FI int warp_f2_stg(int P1, int P2) { return (F_OFF_STG + region2_f2(P1, P2) + 15) / 16 * 16; }
 };
 
 // ---------------------------------------------------------------------------
