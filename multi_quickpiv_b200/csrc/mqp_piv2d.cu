@@ -358,7 +358,8 @@ __device__ __forceinline__ void piv2d_ia(const Piv2dArgs& a, long long ia, float
         }
       }
       __syncwarp();
-#pragma unroll 1
+      // unrolled: a runtime row index would put gv in local memory
+#pragma unroll
       for (int h = 0; h < N / 32; ++h)
         row_process<N, FPRUNE, T, ALG == ALG_ZNCC>(a, sc, pmode, jg[h], gv[h], GH, FH, vmax, mmax, sumsq);
     } else {
@@ -685,11 +686,11 @@ static cudaError_t launch_t(const Piv2dArgs& a, cudaStream_t s, std::string& err
 }
 
 // FP32 FFTCC / NSQECC with staged windows when img2 qualifies.  Measured on
-// B200 (2048^2 vortex, step 8, whole pass): NSQECC interSize 32 2.41 ->
-// 2.31 ms, 24 2.05 -> 1.97, 16 0.86 -> 0.82; FFTCC 32 1.43 -> 1.39, 16 0.65
-// -> 0.52.  ZNCC at interSize 24 ran 2.52 -> 3.23 ms staged (its eight
-// integral-image lookups per lag meet the in-flight copy), so ZNCC loads its
-// rows itself.
+// B200 (2048^2 vortex, step 8, whole pass, results bit-identical): NSQECC
+// interSize 32 2.41 -> 2.22 ms, 24 2.06 -> 1.85, 16 0.86 -> 0.82; FFTCC 32
+// 1.42 -> 1.27, 24 1.32 -> 1.18, 16 0.65 -> 0.52.  ZNCC keeps loading its
+// rows itself (interSize 32 and 16 form their window sums on chip in the
+// space the staged tile would need).
 template <int N, bool FPRUNE, int WARPS, int MINB>
 static bool launch_stg(const Piv2dArgs& a, int alg, cudaStream_t s, std::string& err, cudaError_t& e) {
   if (a.dtype != 0 || !stage_enabled() || (alg != ALG_FFTCC && alg != ALG_NSQECC)) return false;
