@@ -643,12 +643,8 @@ static bool stage_tensor_map(CUtensorMap* m, const void* img, long long H, long 
 // Staged windows are on unless MQP_TUNE_PIV2D_TMA=0 (both kernels give
 // identical results; the knob exists for timing comparisons).
 static bool stage_enabled() {
-  static int on = -1;
-  if (on < 0) {
-    const char* v = getenv("MQP_TUNE_PIV2D_TMA");
-    on = (v && v[0] == '0') ? 0 : 1;
-  }
-  return on == 1;
+  const char* v = getenv("MQP_TUNE_PIV2D_TMA");  // read per launch: a test may switch it between calls
+  return !(v && v[0] == '0');
 }
 
 template <int N, bool FPRUNE, int ALG, typename T, int WARPS, int MINB, bool LW = false, bool STG = false>

@@ -275,3 +275,32 @@ def test_piv2d_window_limits(gpu):
     with pytest.raises(MQPError) as e:  # above 256
         PIV(i1, i2, setPIVParameters(interSize=(64, 64), searchMargin=(100, 100), step=(64, 64)))
     assert e.value.code == _lib.MQP_ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("alg", ["fft", "nsqecc"])
+@pytest.mark.parametrize("shape,IS,SM,st,thr", [((160, 144), 32, 16, 8, -1.0), ((258, 250), 32, 16, 8, -1.0),
+                                                ((203, 177), 16, 8, 4, -1.0), ((96, 100), 32, 10, 16, 0.0),
+                                                ((300, 260), 24, 12, 6, -1.0), ((68, 64), 32, 16, 4, -1.0)],
+                         ids=["base", "h_not_mult4", "odd", "thr", "is24", "small"])
+def test_staged_windows_equal_unstaged(alg, shape, IS, SM, st, thr, gpu, monkeypatch):
+    """FP32 FFTCC / NSQECC stage each warp's next search window into shared
+    memory by TMA (68 x 64 tile, row start rounded down to 4 pixels, zero
+    fill outside the image); images whose row pitch is not a multiple of 16
+    bytes take the unstaged kernel.  Both give the same vector field bit for
+    bit, borders and skipped IAs included."""
+    import torch
+    i1, i2, _ = synth.pair_2d_shift(shape=shape, shift=(3.7, -2.2), seed_stream=31, dtype=np.float32)
+    i1 = i1.copy()
+    if thr >= 0:
+        i1[:40, :40] = -1.0
+    p = setPIVParameters(corr_alg=alg, interSize=(IS, IS), searchMargin=(SM, SM), step=(st, st), computeSN=True,
+                         threshold=thr)
+    d1, d2 = torch.from_numpy(i1).cuda(), torch.from_numpy(i2).cuda()
+    out = {}
+    for mode in ("1", "0"):
+        monkeypatch.setenv("MQP_TUNE_PIV2D_TMA", mode)
+        VF, SN = PIV(d1, d2, p)
+        out[mode] = (VF.cpu().numpy(), SN.cpu().numpy())
+    assert np.array_equal(out["1"][0], out["0"][0], equal_nan=True)
+    assert np.array_equal(out["1"][1], out["0"][1], equal_nan=True)
+    assert np.isfinite(out["1"][0]).all()
