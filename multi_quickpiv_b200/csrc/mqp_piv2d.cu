@@ -268,9 +268,12 @@ __device__ __forceinline__ void piv2d_ia(const Piv2dArgs& a, long long ia, float
   constexpr int M = N / 2;
   constexpr bool MASKED = ALG == ALG_MASK_NSQECC;
   static_assert(!LW || ((ALG == ALG_ZNCC || ALG == ALG_NSQECC) && FPRUNE), "on-chip window sums: ZNCC / NSQECC");
-  static_assert(!STG || (!LW && !MASKED && sizeof(T) == 4), "staged windows: FP32, unmasked, integral-image sums");
+  static_assert(!STG || (!MASKED && sizeof(T) == 4), "staged windows: FP32, unmasked");
   const int P1 = 2 * a.SM1 + 1, P2 = 2 * a.SM2 + 1;
-  float2* FH = GH + (LW ? Lay::F_OFF_LW : (STG ? Lay::F_OFF_STG : Lay::F_OFF));
+  // the plane follows the largest user of the G region: spectra, the window-sum table, the staged tile
+  constexpr int F_OFF = STG ? (LW && Lay::F_OFF_LW > Lay::F_OFF_STG ? Lay::F_OFF_LW : Lay::F_OFF_STG)
+                            : (LW ? Lay::F_OFF_LW : Lay::F_OFF);
+  float2* FH = GH + F_OFF;
   // the next IA's window into the dead G spectra (every lane calls it)
   auto stage_next = [&]() {
     if (STG && ia_next >= 0 && *phase != STAGE_OFF) {
@@ -447,7 +450,7 @@ __device__ __forceinline__ void piv2d_ia(const Piv2dArgs& a, long long ia, float
       for (int s2 = lane; s2 < P2; s2 += 32)
         plane[s1 * P2 + s2] = (double)tail_row_value<N, FPRUNE>(GH, tw, s1, s2) * scale;
     __syncwarp();
-    stage_next();
+    if (!LW) stage_next();  // with LW the table holds the G region until the finish has read it
     if (LW) {
       // the G spectra are dead: their space takes the window-sum table
       lw_rows<N, T, ALG == ALG_ZNCC>(a, g, sc.meanG, lane, P2, lw);
@@ -502,6 +505,7 @@ __device__ __forceinline__ void piv2d_ia(const Piv2dArgs& a, long long ia, float
       acc_take(acc, R, s1, s2, P1, e);
     }
   __syncwarp();
+  if (LW) stage_next();
   double best = acc.best;
   int bidx = acc.bidx;
   warp_peak(best, bidx);
@@ -539,7 +543,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) piv2d_kernel(Piv2dArgs a, co
   constexpr bool MASKED = ALG == ALG_MASK_NSQECC;
   const int P1 = 2 * a.SM1 + 1, P2 = 2 * a.SM2 + 1;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int wf2 = LW ? Lay::warp_f2_lw(P1, P2) : (STG ? Lay::warp_f2_stg(P1, P2) : Lay::warp_f2(P1, P2, MASKED));
+  const int wf2 = STG ? Lay::warp_f2_stg(P1, P2) : (LW ? Lay::warp_f2_lw(P1, P2) : Lay::warp_f2(P1, P2, MASKED));
   float2* GH = smem + (size_t)warp * wf2;
   float2* tw = smem + (size_t)WARPS * wf2;  // (cos, sin)(2 pi j / N)
   uint64_t* mbar = reinterpret_cast<uint64_t*>(tw + N) + warp;
@@ -651,7 +655,7 @@ template <int N, bool FPRUNE, int ALG, typename T, int WARPS, int MINB, bool LW 
 static cudaError_t launch_t(const Piv2dArgs& a, cudaStream_t s, std::string& err, const CUtensorMap* tm = nullptr) {
   using Lay = Layout2d<N, FPRUNE>;
   const int P1 = 2 * a.SM1 + 1, P2 = 2 * a.SM2 + 1;
-  const int wf2 = LW ? Lay::warp_f2_lw(P1, P2) : (STG ? Lay::warp_f2_stg(P1, P2) : Lay::warp_f2(P1, P2, ALG == ALG_MASK_NSQECC));
+  const int wf2 = STG ? Lay::warp_f2_stg(P1, P2) : (LW ? Lay::warp_f2_lw(P1, P2) : Lay::warp_f2(P1, P2, ALG == ALG_MASK_NSQECC));
   const size_t smem = ((size_t)WARPS * wf2 + N + (STG ? WARPS : 0)) * sizeof(float2);
   auto kern = piv2d_kernel<N, FPRUNE, ALG, T, WARPS, MINB, LW, STG>;
   CUtensorMap tmap;
@@ -681,19 +685,19 @@ static cudaError_t launch_t(const Piv2dArgs& a, cudaStream_t s, std::string& err
   return e;
 }
 
-// FP32 FFTCC / NSQECC with staged windows when img2 qualifies.  Measured on
-// B200 (2048^2 vortex, step 8, whole pass, results bit-identical): NSQECC
-// interSize 32 2.41 -> 2.22 ms, 24 2.06 -> 1.85, 16 0.86 -> 0.82; FFTCC 32
-// 1.42 -> 1.27, 24 1.32 -> 1.18, 16 0.65 -> 0.52.  ZNCC keeps loading its
-// rows itself (interSize 32 and 16 form their window sums on chip in the
-// space the staged tile would need).
+// FP32 FFTCC / NSQECC / ZNCC with staged windows when img2 qualifies.
+// Measured on B200 (2048^2 vortex, step 8, whole pass, results
+// bit-identical): NSQECC interSize 32 2.41 -> 2.22 ms, 24 2.06 -> 1.85, 16
+// 0.86 -> 0.82; FFTCC 32 1.42 -> 1.27, 24 1.32 -> 1.18, 16 0.65 -> 0.52;
+// ZNCC 24 2.55 -> 2.49 (ZNCC with interSize N/2 goes through launch_lw).
 template <int N, bool FPRUNE, int WARPS, int MINB>
 static bool launch_stg(const Piv2dArgs& a, int alg, cudaStream_t s, std::string& err, cudaError_t& e) {
-  if (a.dtype != 0 || !stage_enabled() || (alg != ALG_FFTCC && alg != ALG_NSQECC)) return false;
+  if (a.dtype != 0 || !stage_enabled() || (alg != ALG_FFTCC && alg != ALG_NSQECC && alg != ALG_ZNCC)) return false;
   CUtensorMap tm;
   if (!stage_tensor_map(&tm, a.img2, a.H, a.W, N)) return false;
-  e = alg == ALG_FFTCC ? launch_t<N, FPRUNE, ALG_FFTCC, float, WARPS, MINB, false, true>(a, s, err, &tm)
-                       : launch_t<N, FPRUNE, ALG_NSQECC, float, WARPS, MINB, false, true>(a, s, err, &tm);
+  e = alg == ALG_FFTCC  ? launch_t<N, FPRUNE, ALG_FFTCC, float, WARPS, MINB, false, true>(a, s, err, &tm)
+      : alg == ALG_ZNCC ? launch_t<N, FPRUNE, ALG_ZNCC, float, WARPS, MINB, false, true>(a, s, err, &tm)
+                        : launch_t<N, FPRUNE, ALG_NSQECC, float, WARPS, MINB, false, true>(a, s, err, &tm);
   return true;
 }
 
@@ -737,6 +741,11 @@ static cudaError_t launch_lw(const Piv2dArgs& a, int alg, cudaStream_t s, std::s
     err = "on-chip window sums are built for ZNCC";
     return cudaErrorInvalidValue;
   }
+  // staged windows as well at length 32 (interSize 16: 0.98 -> 0.86 ms per 2048^2 pass); at length 64
+  // the tile can only be issued after the finish has read the table, and the pass ran 2.77 -> 3.09 ms
+  CUtensorMap tm;
+  if (N == 32 && a.dtype == 0 && stage_enabled() && stage_tensor_map(&tm, a.img2, a.H, a.W, N))
+    return launch_t<N, true, ALG_ZNCC, float, 4, MINB, true, true>(a, s, err, &tm);
   return a.dtype == 0 ? launch_t<N, true, ALG_ZNCC, float, 4, MINB, true>(a, s, err)
                       : launch_t<N, true, ALG_ZNCC, double, 4, MINB, true>(a, s, err);
 }

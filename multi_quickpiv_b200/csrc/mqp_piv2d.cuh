@@ -169,6 +169,7 @@ struct Layout2d {
   static constexpr int TILE_F2 = ((N + 4) * N + 1) / 2;
   static constexpr int F_OFF_STG = G_SIZE > TILE_F2 ? G_SIZE : TILE_F2;
   static MQP_HD MQP_FI int warp_f2_stg(int P1, int P2) { return (F_OFF_STG + region2_f2(P1, P2) + 15) / 16 * 16; }
+  static_assert(F_OFF_STG >= F_OFF_LW, "the staged layout also holds the window-sum table");
 };
 
 // ---------------------------------------------------------------------------
