@@ -277,13 +277,13 @@ def test_piv2d_window_limits(gpu):
     assert e.value.code == _lib.MQP_ERR_UNSUPPORTED
 
 
-@pytest.mark.parametrize("alg", ["fft", "nsqecc"])
+@pytest.mark.parametrize("alg", ["fft", "nsqecc", "zncc"])
 @pytest.mark.parametrize("shape,IS,SM,st,thr", [((160, 144), 32, 16, 8, -1.0), ((258, 250), 32, 16, 8, -1.0),
                                                 ((203, 177), 16, 8, 4, -1.0), ((96, 100), 32, 10, 16, 0.0),
                                                 ((300, 260), 24, 12, 6, -1.0), ((68, 64), 32, 16, 4, -1.0)],
                          ids=["base", "h_not_mult4", "odd", "thr", "is24", "small"])
 def test_staged_windows_equal_unstaged(alg, shape, IS, SM, st, thr, gpu, monkeypatch):
-    """FP32 FFTCC / NSQECC stage each warp's next search window into shared
+    """FP32 FFTCC / NSQECC / ZNCC stage each warp's next search window into shared
     memory by TMA (68 x 64 tile, row start rounded down to 4 pixels, zero
     fill outside the image); images whose row pitch is not a multiple of 16
     bytes take the unstaged kernel.  Both give the same vector field bit for
