@@ -184,7 +184,7 @@ int run_pass_2d(mqp_ctx* ctx, const Problem& pb, const mqp_params* p, const void
   if (rc != MQP_OK) return rc;
   mqp::Piv2dArgs a = args_2d(ctx, pb, p, d1, d2, dmask, dskip, dtype, dVF, dSN, dpred, dplanes, ia_begin, ia_end);
   if (huge) {
-    cudaError_t e = ctx->huge.ensure(mqp::piv2d_huge_scratch_bytes(ctx->device));
+    cudaError_t e = ctx->huge.ensure(mqp::piv2d_huge_scratch_bytes(ctx->device, 2 * pb.SM[0] + 1, 2 * pb.SM[1] + 1));
     if (e != cudaSuccess) return cuda_fail(ctx, e, "scratch of the 2D kernel for search windows above 128");
     a.huge = (float2*)ctx->huge.ptr;
     std::string err;

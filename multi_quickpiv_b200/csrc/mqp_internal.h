@@ -70,12 +70,12 @@ cudaError_t launch_piv2d_batch(const Piv2dBatch& b, cudaStream_t s, std::string&
 // Search windows of 129..256 (FFT length 256, interrogation windows up to
 // 128, FFTCC / ZNCC / NSQECC): one 256-thread block per IA over a scratch
 // slot per resident block (mqp_piv2d_huge.cu); a.huge must point at
-// piv2d_huge_scratch_bytes(device) bytes.
+// piv2d_huge_scratch_bytes(device, P1, P2) bytes.
 bool piv2d_huge_ok(int SS1, int SS2, int IS1, int IS2, int alg);
 // ZNCC passes whose kernel forms the window sums on chip: they need no
 // integral image of img2^2 (mqp_piv2d.cu).
 bool piv2d_local_sums(int IS1, int IS2, int SM1, int SM2, int alg);
-size_t piv2d_huge_scratch_bytes(int device);
+size_t piv2d_huge_scratch_bytes(int device, int P1, int P2);
 cudaError_t launch_piv2d_huge(const Piv2dArgs& a, int alg, cudaStream_t s, std::string& err);
 
 // Team variant of the fused 2D kernel (mqp_piv2d_team.cu): one IA per team

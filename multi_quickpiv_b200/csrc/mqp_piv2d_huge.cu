@@ -45,11 +45,12 @@ __device__ __forceinline__ void huge_ia(const Piv2dArgs& a, long long ia, float2
   constexpr bool ZN = ALG == ALG_ZNCC;
   const int P1 = 2 * a.SM1 + 1, P2 = 2 * a.SM2 + 1;
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-  float2* GS = slot + HugeSlot::GS_OFF;
-  float2* FS = slot + HugeSlot::FS_OFF;
-  float2* LG = slot + HugeSlot::LG_OFF;
-  float* cc = reinterpret_cast<float*>(slot + HugeSlot::CC_OFF);
-  double* plane = reinterpret_cast<double*>(slot + HugeSlot::PL_OFF);
+  const HugeSlot L(P1, P2);
+  float2* GS = slot + L.gs;
+  float2* FS = slot + L.fs;
+  float2* LG = slot + L.lg;
+  float* cc = reinterpret_cast<float*>(slot + L.cc);
+  double* plane = reinterpret_cast<double*>(slot + L.pl);
   float2* park = sm;
   float2* pack = sm + HugeSmem::PARK;
   const float2* tw = pack + HugeSmem::PACK;
@@ -203,7 +204,7 @@ __global__ void __launch_bounds__(HUGE_THREADS, 1) piv2d_huge_kernel(Piv2dArgs a
   float2* tw = sm + HugeSmem::PARK + HugeSmem::PACK;
   for (int j = threadIdx.x; j < NH; j += blockDim.x) tw[j] = twiddle_rt(j * (TW_N / NH));
   __syncthreads();
-  float2* slot = a.huge + (long long)blockIdx.x * HugeSlot::TOTAL;
+  float2* slot = a.huge + (long long)blockIdx.x * HugeSlot(2 * a.SM1 + 1, 2 * a.SM2 + 1).total;
   for (long long ia = a.ia_begin + blockIdx.x; ia < a.ia_end; ia += gridDim.x) huge_ia<ALG, T>(a, ia, slot, sm);
 }
 
@@ -245,8 +246,8 @@ bool piv2d_huge_ok(int SS1, int SS2, int IS1, int IS2, int alg) {
   return SS > 128 && SS <= NH && IS1 <= MH && IS2 <= MH && (alg == ALG_FFTCC || alg == ALG_ZNCC || alg == ALG_NSQECC);
 }
 
-size_t piv2d_huge_scratch_bytes(int device) {
-  return (size_t)device_sm_count(device) * (size_t)HugeSlot::TOTAL * sizeof(float2);
+size_t piv2d_huge_scratch_bytes(int device, int P1, int P2) {
+  return (size_t)device_sm_count(device) * (size_t)HugeSlot(P1, P2).total * sizeof(float2);
 }
 
 cudaError_t launch_piv2d_huge(const Piv2dArgs& a, int alg, cudaStream_t s, std::string& err) {

@@ -33,14 +33,21 @@ constexpr int MH = NH / 2;       // packed spectrum columns, complex row length
 constexpr int QH = 64;           // register FFT length of every split transform
 constexpr int HUGE_THREADS = 256;
 
-// Per-block scratch slot (float2 units): GS | FS | LG | CC | PL
+// Per-block scratch slot (float2 units), sized for the pass's lags so that
+// all resident blocks' slots stay in L2:
+//   stages A-B  LG [k2][s1] (128 x P1) | GS [k2][x1] (128 x 256) | FS [k2][x1] (128 x 128)
+//   stages C-D  LG | CC (P1 P2 floats, over the dead GS) | PL (P1 P2 doubles, after CC)
 struct HugeSlot {
-  static constexpr long long GS_OFF = 0, GS = (long long)MH * NH;       // [k2][x1], x1 < 256
-  static constexpr long long FS_OFF = GS_OFF + GS, FS = (long long)MH * MH;  // [k2][x1], x1 < 128
-  static constexpr long long LG_OFF = FS_OFF + FS, LG = (long long)MH * NH;  // [k2][s1]
-  static constexpr long long CC_OFF = LG_OFF + LG, CC = (long long)NH * NH / 2;  // floats: P1 P2 <= 65536
-  static constexpr long long PL_OFF = CC_OFF + CC, PL = (long long)NH * NH;  // doubles: P1 P2
-  static constexpr long long TOTAL = PL_OFF + PL;
+  long long lg, gs, fs, cc, pl, total;
+  MQP_HD HugeSlot(int P1, int P2) {
+    lg = 0;
+    gs = (long long)MH * P1;
+    fs = gs + (long long)MH * NH;
+    cc = gs;
+    pl = cc + ((long long)P1 * P2 + 1) / 2;
+    const long long ab = fs + (long long)MH * MH, cd = pl + (long long)P1 * P2;
+    total = ((ab > cd ? ab : cd) + 15) / 16 * 16;  // slots on 128-byte boundaries
+  }
 };
 
 // Shared memory (float2 units): the park/exchange area of stage B (64
@@ -255,7 +262,7 @@ MQP_HD MQP_FI void huge_col_inverse(int q, float2* park, const float2* tw) {
 
 // Part 4 (after the quad's exchange): lags s1 = s + 64 p of the column,
 //   x[s + 64p] = sum_q W_4^{-pq} xch[q][s],   xch[q][s] = xch[s * HPS + q * 64],
-// those below P1 to LG[k2 * 256 + s1].
+// those below P1 to LG[k2 * P1 + s1].
 MQP_HD MQP_FI void huge_col_combine(int k2, int p, int P1, const float2* xch, float2* LG) {
 #pragma unroll 4
   for (int s = 0; s < QH; ++s) {
@@ -269,7 +276,7 @@ MQP_HD MQP_FI void huge_col_combine(int k2, int p, int P1, const float2* xch, fl
     else if (p == 1) v = cadd(csub(a0, a2), cmul_pi(csub(a1, a3)));
     else if (p == 2) v = csub(cadd(a0, a2), cadd(a1, a3));
     else v = cadd(csub(a0, a2), cmul_mi(csub(a1, a3)));
-    LG[(long long)k2 * NH + s1] = v;
+    LG[(long long)k2 * P1 + s1] = v;
   }
 }
 
@@ -307,11 +314,11 @@ MQP_HD MQP_FI void huge_b_part3(int r, int t, int P1, const float2* park, float2
 // ---------------------------------------------------------------------------
 // stage C: lag row s1, half hh of the complex-to-real inverse along k2
 // ---------------------------------------------------------------------------
-// As team_phase3_row with the row's spectrum X[u] = LG[u * 256 + s1].
+// As team_phase3_row with the row's spectrum X[u] = LG[u * P1 + s1].
 MQP_HD MQP_FI void huge_lag_row(int s1, int hh, int P1, int P2, const float2* LG, float* cc, float scale) {
   mqp_no_hoist();
   constexpr int M = MH, Q = QH;
-  auto X = [&](int u) { return LG[(long long)u * NH + s1]; };
+  auto X = [&](int u) { return LG[(long long)u * P1 + s1]; };
   auto tk = [](float2 A, float2 Bm, int k) {
     const float2 B = cconj(Bm);
     const float2 E = cadd(A, B);

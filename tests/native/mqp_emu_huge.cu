@@ -17,11 +17,12 @@ template <int ALG, typename T>
 static void emu_huge_ia(const Piv2dArgs& a, long long ia, float2* slot, float2* sm) {
   constexpr bool ZN = ALG == ALG_ZNCC;
   const int P1 = 2 * a.SM1 + 1, P2 = 2 * a.SM2 + 1;
-  float2* GS = slot + HugeSlot::GS_OFF;
-  float2* FS = slot + HugeSlot::FS_OFF;
-  float2* LG = slot + HugeSlot::LG_OFF;
-  float* cc = reinterpret_cast<float*>(slot + HugeSlot::CC_OFF);
-  double* plane = reinterpret_cast<double*>(slot + HugeSlot::PL_OFF);
+  const HugeSlot L(P1, P2);
+  float2* GS = slot + L.gs;
+  float2* FS = slot + L.fs;
+  float2* LG = slot + L.lg;
+  float* cc = reinterpret_cast<float*>(slot + L.cc);
+  double* plane = reinterpret_cast<double*>(slot + L.pl);
   float2* park = sm;
   float2* pack = sm + HugeSmem::PARK;
   const float2* tw = pack + HugeSmem::PACK;
@@ -96,7 +97,7 @@ static void emu_huge_ia(const Piv2dArgs& a, long long ia, float2* slot, float2* 
 
 template <int ALG>
 static void emu_huge_run(const Piv2dArgs& a) {
-  std::vector<float2> slot((size_t)HugeSlot::TOTAL), sm((size_t)HugeSmem::TOTAL);
+  std::vector<float2> slot((size_t)HugeSlot(2 * a.SM1 + 1, 2 * a.SM2 + 1).total), sm((size_t)HugeSmem::TOTAL);
   float2* tw = sm.data() + HugeSmem::PARK + HugeSmem::PACK;
   for (int j = 0; j < NH; ++j) tw[j] = twiddle_rt(j * (TW_N / NH));
   for (long long ia = a.ia_begin; ia < a.ia_end; ++ia) {
