@@ -5,7 +5,9 @@ vortex pair with ramp and gain, interSize 32, searchMargin 16, step 8 (64,009
 IAs per pair), NSQECC (the reference's default algorithm; --alg zncc for
 ZNCC).  --workload shear3d: the 512x512x256 Float32 volume pair (uniform shift
 plus du/dz shear), FFTCC, interSize 32^3, searchMargin 16^3, step 16^3 (14,415
-IAs).  One step = one PIV of one image pair.
+IAs).  --workload window256: the vortex pair at interSize 128, searchMargin
+64, step 32 (search windows of 256, the coarsest pass of a 3-level refinement
+from interSize 32; 3,721 IAs at 2048^2).  One step = one PIV of one image pair.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload W]
 
@@ -152,6 +154,13 @@ class Workload:
             self.alg = "fft"
             self.IS, self.SM, self.step = 32, 16, 16
             self.desc = "shear pair 512x512x256 float32, fft, IS 32 SM 16 step 16"
+        elif args.workload == "window256":
+            # search windows of 256 (interSize 128, margin 64: the coarsest pass of a 3-level
+            # refinement from interSize 32), 2D vortex pair, step 32
+            self.i1, self.i2, _ = synth.pair_2d_vortex(shape=(args.size, args.size))
+            self.alg = args.alg
+            self.IS, self.SM, self.step = 128, 64, 32
+            self.desc = f"vortex pair {args.size}x{args.size} float32, {args.alg}, IS 128 SM 64 step 32"
         else:
             self.i1, self.i2, _ = synth.pair_2d_vortex(shape=(args.size, args.size))
             self.alg = args.alg
@@ -165,7 +174,8 @@ class Workload:
         self.vf = tuple((n - self.IS) // self.step + 1 for n in self.i1.shape)
         self.n_ia = int(np.prod(self.vf))
         norm = self.alg != "fft"
-        self.flop_per_ia = flops_per_ia(cs=64, P=2 * self.SM + 1, IS=self.IS, norm=norm, nd=self.nd)
+        self.fft_len = 256 if args.workload == "window256" else 64
+        self.flop_per_ia = flops_per_ia(cs=self.fft_len, P=2 * self.SM + 1, IS=self.IS, norm=norm, nd=self.nd)
         npx = int(np.prod(self.i1.shape))
         ii = int(np.prod([n + 1 for n in self.i1.shape])) * 8
         # algorithmic bytes of one pass: both images once, the FP64 integral
@@ -319,6 +329,8 @@ def run_ours(args):
     achieved = wl.flop_per_ia * n_ia / (kern_ms / 1e3)
     traffic = None
     tfile = "piv2d_traffic.json" if nd == 2 else "piv3d_traffic.json"
+    if wl.name == "window256":
+        tfile = "piv2d_huge_traffic.json"
     try:
         with open(os.path.join(ROOT, "profiles", tfile)) as f:
             tr = json.load(f)
@@ -328,6 +340,8 @@ def run_ours(args):
         pass
     kname = ("piv2d_kernel (one IA per warp, FFT length 64, search windows staged by TMA)" if nd == 2
              else "k3a_kernel + k3b_kernel + k3c_kernel (all chunks of one pass)")
+    if wl.name == "window256":
+        kname = "piv2d_huge_kernel (one 256-thread block per IA, FFT length 256)"
     roof = {"bound": "fp32", "kernel": kname, "achieved": achieved / 1e12, "peak": fp32_peak / 1e12,
             "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": traffic,
             "traffic_unit": f"bytes per pass (ncu dram__bytes_read+write, profiles/{tfile})",
@@ -638,8 +652,9 @@ def main(argv=None):
     ap.add_argument("--size", type=int, default=2048)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ref-budget", type=float, default=10.0)
-    ap.add_argument("--workload", default="vortex2048", choices=["vortex2048", "shear3d", "batch64", "serve"],
-                    help="vortex2048: 2D vortex pair (--size, --alg); shear3d: 512x512x256 FFTCC volumes; "
+    ap.add_argument("--workload", default="vortex2048", choices=["vortex2048", "shear3d", "batch64", "serve", "window256"],
+                    help="vortex2048: 2D vortex pair (--size, --alg); window256: the same pair at interSize 128, "
+                         "margin 64, step 32 (search windows of 256); shear3d: 512x512x256 FFTCC volumes; "
                          "batch64: 64 mixed pairs with 3-pass refinement (batch plans vs per-pair calls); "
                          "serve: Poisson request streams (latency p50/p99; --steps = requests)")
     ap.add_argument("--chunk3d", type=int, default=0, help="IAs per 3D chunk (0: autotuned in warm-up)")
