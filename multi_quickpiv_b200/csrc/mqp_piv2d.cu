@@ -624,16 +624,15 @@ static bool stage_tensor_map(CUtensorMap* m, const void* img, long long H, long 
   typedef CUresult (*EncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-  static EncodeTiled encode = nullptr;
-  static bool looked = false;
-  if (!looked) {
+  // looked up once (thread-safe static initialisation: serving launches from several threads)
+  static const EncodeTiled encode = []() -> EncodeTiled {
     void* fn = nullptr;
     cudaDriverEntryPointQueryResult q;
     if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
         q == cudaDriverEntryPointSuccess)
-      encode = (EncodeTiled)fn;
-    looked = true;
-  }
+      return (EncodeTiled)fn;
+    return nullptr;
+  }();
   if (!encode) return false;
   const cuuint64_t dims[2] = {(cuuint64_t)H, (cuuint64_t)W};
   const cuuint64_t strides[1] = {(cuuint64_t)H * 4};
